@@ -1,0 +1,319 @@
+"""Benchmark of the peptide-search query path (spectra/s) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload open-20k] [--impl ours|reference]
+
+A step is one search of the whole synthetic batch (default: the open-search
+workload -- 20,000 proteins, Met oxidation <= 2, b/y ions of charge 1-2, 50,000
+spectra of 30-150 peaks, +-500 Da precursor window, +-0.05 Da fragment tolerance,
+top-K 5).  The index (1.3 GB of ion ids) is larger than L2, so steps run back to
+back without an L2 flush.
+
+Printed (rank 0, one JSON line): value = spectra/s with queries resident in HBM
+(CUDA events on the launching stream, max over ranks); e2e = spectra/s through
+the host-buffer API (pinned host queries in, results out, per step); roofline of
+the dominant kernel against the measured HBM copy bandwidth; cpu_baseline = the
+reference's own OpenMP CPU query path timed on a bounded sample on this host.
+
+Under torchrun each rank searches its own batch against a replica of the index
+(spectra are independent: weak scaling, no collective on the data path).
+``--impl reference`` times the reference's CPU implementation alone (rank 0).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "open-20k": dict(nproteins=20000, db_seed=1, maxz=2, mods=[("M", 15.9949, 2)], nmods=2, nspec=50000, dM=500.0,
+                     q=dict(charges=(2, 4), frag_charge2=True, keep_p=(0.6, 0.6), noise_mode="fill",
+                            npeaks_range=(30, 150))),
+    "closed-1k": dict(nproteins=1000, db_seed=1, maxz=1, mods=[], nmods=0, nspec=2000, dM=10.0,
+                      q=dict(charges=(2, 3), frag_charge2=False, keep_p=(0.6, 0.6), noise_mode="fixed40")),
+}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def make_workload(name: str, rank: int):
+    import gicops_b200 as gx
+    w = WORKLOADS[name]
+    t = time.time()
+    db = gx.synth.make_database(w["nproteins"], seed=w["db_seed"])
+    H = gx.HostIndex.build(db, maxz=w["maxz"], mods=w["mods"], nmods=w["nmods"])
+    q = gx.synth.make_queries(H.entries_by_len(), w["nspec"], seed=1000 + rank, **w["q"])
+    log(f"[bench] workload {name}: {H.total_entries()} entries, {H.total_ions()} ion ids, {q.n} spectra, "
+        f"{len(q.moz)} peaks ({time.time() - t:.1f}s)")
+    return w, db, H, q
+
+
+def smi_id(local: int) -> str:
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        ids = [x.strip() for x in vis.split(",") if x.strip()]
+        if local < len(ids):
+            return ids[local]
+    return str(local)
+
+
+def sample_clocks(stop: threading.Event, out: list, gpu: int):
+    cmd = ["nvidia-smi", f"--id={smi_id(gpu)}", "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+           "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+           "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits",
+           "-lms", "200"]
+    try:
+        p = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+    except OSError:
+        return
+    try:
+        while not stop.is_set():
+            line = p.stdout.readline()
+            if not line:
+                break
+            out.append([x.strip() for x in line.split(",")])
+    finally:
+        p.terminate()
+        p.wait()
+
+
+def summarize_clocks(rows: list) -> dict:
+    if not rows:
+        return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+    sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+    mx = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    reasons = sorted({names[i] for r in rows for i in range(4) if len(r) > 4 + i and r[4 + i].lower() == "active"})
+    return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+            "reasons": reasons, "samples": len(rows)}
+
+
+def reference_cpu(w: dict, db, q, steps: int, warmup: int, sample: int | None = None):
+    """The reference's OpenMP CPU query path (oracle/_ref/ref_harness) on a sample of q."""
+    harness = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+    cores = os.cpu_count() or 1
+    if sample is None:
+        sample = int(min(q.n, max(2048, min(16384, 128 * cores))))
+    sel = np.random.Generator(np.random.PCG64(7)).choice(q.n, size=sample, replace=False)
+    sel.sort()
+    sq = q.subset(sel)
+    with tempfile.TemporaryDirectory() as tmp:
+        dbdir = os.path.join(tmp, "db")
+        db.write_peps(dbdir)
+        qf = os.path.join(tmp, "q.pbin")
+        sq.write_pbin(qf)
+        cmd = [harness, "--db", dbdir, "--maxz", str(w["maxz"]), "--dM", str(w["dM"]), "--dF", "5",
+               "--threads", str(cores), "--topmatches", "5", "--queries", qf, "--repeat", str(warmup + steps)]
+        for r, m, n in w["mods"]:
+            cmd += ["--mods", f"{r}:{m}:{n}"]
+        if w["mods"]:
+            cmd += ["--nmods", str(w["nmods"])]
+        t = time.time()
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"reference harness failed: {r.stderr[-400:]}")
+        rec = json.loads(r.stdout.strip().splitlines()[-1])
+    each = rec["query_s_each"][warmup:]
+    per = float(np.mean(each))
+    log(f"[bench] reference CPU: {sample} spectra x {len(rec['query_s_each'])} repeats, {per:.3f} s each, "
+        f"index build {rec['index_s']:.1f}s ({time.time() - t:.1f}s total)")
+    return dict(value=sample / per, cores=cores, sample=sample, seconds=per, steps=len(each))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="open-20k", choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    metric = "query spectra/s"
+    unit = "spectra/s"
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        w, db, H, q = make_workload(args.workload, 0)
+        ref = reference_cpu(w, db, q, args.steps, args.warmup)
+        line = {"metric": metric, "value": ref["value"], "unit": unit, "impl": "reference", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ref["seconds"] * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32+f64",
+                "data": "synthetic (seeded generator)",
+                "config": {"workload": args.workload, "spectra_per_step": ref["sample"], "window_da": w["dM"]},
+                "cpu_baseline": {"value": ref["value"], "unit": unit, "cores": ref["cores"], "kind": "reference",
+                                 "sample": f"{ref['sample']} of the workload's {w['nspec']} spectra per step"},
+                "e2e": {"value": ref["value"], "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    import gicops_b200 as gx
+    from gicops_b200.search import algorithmic_bytes
+    import gicops_b200._native as N
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    w, db, H, q = make_workload(args.workload, rank)
+    params = gx.SearchParams(dM=w["dM"], dF=5, topmatches=5, expect_max=20.0)
+    dev = gx.DeviceIndex(H, local)
+    ws = gx.Searcher(dev, q.n, len(q.moz))
+    stream = torch.cuda.current_stream()
+    d = torch.device("cuda", local)
+    t_idx = torch.from_numpy(q.idx.view(np.int32).copy()).to(d)
+    t_moz = torch.from_numpy(q.moz.copy()).to(d)
+    t_int = torch.from_numpy(q.intn.copy()).to(d)
+    t_pre = torch.from_numpy(q.prec.copy()).to(d)
+    t_out = torch.empty(q.n * N.RESULT_DTYPE.itemsize, dtype=torch.uint8, device=d)
+    qd = dict(nspec=q.n, npeaks=len(q.moz), idx=t_idx.data_ptr(), moz=t_moz.data_ptr(), intn=t_int.data_ptr(),
+              prec=t_pre.data_ptr())
+
+    def step():
+        ws.search_device(qd, params, t_out.data_ptr(), stream=stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    # ---- timed region (device events, queries resident in HBM) ---------------------
+    clocks, stop = [], threading.Event()
+    th = threading.Thread(target=sample_clocks, args=(stop, clocks, local), daemon=True)
+    th.start()
+    time.sleep(0.5)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    n0 = gx.lib().gx_launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    launches = int(gx.lib().gx_launch_count() - n0)
+    ms = e0.elapsed_time(e1)
+    stop.set()
+    th.join(timeout=5)
+    if dist:
+        t = torch.tensor([ms], device=d)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    value = q.n * world / (ms_step / 1e3)
+
+    # ---- dominant kernel duration (events around each launch, same stream) --------
+    gx.lib().gx_profile_enable(1)
+    for _ in range(args.steps):
+        step()
+    torch.cuda.synchronize()
+    kt = N.kernel_times()
+    gx.lib().gx_profile_enable(0)
+    top_k = max(kt, key=lambda k: kt[k][1])
+    k_ms = kt[top_k][1] / kt[top_k][0]
+
+    # ---- end to end through the host-buffer API ------------------------------------
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    qp = gx.synth.QueryBatch(pin(q.idx), pin(q.moz), pin(q.intn), pin(q.prec), pin(q.charge), q.rtime)
+    out_pinned = torch.empty(q.n * N.RESULT_DTYPE.itemsize, dtype=torch.uint8).pin_memory().numpy()
+    from gicops_b200.search import make_c_queries
+    import ctypes as C
+    cq, keep = make_c_queries(qp, params)
+    cp = params.c()
+
+    def e2e_step():
+        N.check(gx.lib().gx_search_host(dev.handle, ws.handle, C.byref(cq), C.byref(cp), out_pinned.ctypes.data,
+                                        None, None))
+
+    for _ in range(2):
+        e2e_step()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    if dist:
+        t = torch.tensor([e2e_s], device=d)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    h2d = q.idx.nbytes + q.moz.nbytes + q.intn.nbytes + q.prec.nbytes
+    d2h = q.n * N.RESULT_DTYPE.itemsize + 4
+
+    # ---- roofline numerator: algorithmic bytes of one launch ------------------------
+    rs = np.random.Generator(np.random.PCG64(3)).choice(q.n, size=min(q.n, 4096), replace=False)
+    ab = algorithmic_bytes(H, q.subset(np.sort(rs)), params)
+    bytes_launch = float(ab.mean()) * q.n
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = bytes_launch / (k_ms / 1e3) / 1e9
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tf):
+        tj = json.load(open(tf))
+        ent = tj.get(args.workload, {}).get(top_k)
+        if ent:
+            traffic = ent["dram_bytes_per_launch"]
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            ref = reference_cpu(w, db, q, steps=1, warmup=1)
+            cpu = {"value": ref["value"], "unit": unit, "cores": ref["cores"], "kind": "reference",
+                   "sample": f"{ref['sample']} of {q.n} spectra, reference DSLIM_QuerySpectrum, "
+                             f"all {ref['cores']} host threads, query time only"}
+        except Exception as ex:  # the checker binary may be absent on a machine without the reference build
+            log(f"[bench] reference CPU baseline unavailable: {ex}")
+
+    if rank == 0:
+        line = {
+            "metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32+f64", "data": "synthetic (seeded generator, no dataset)",
+            "config": {"workload": args.workload, "spectra_per_gpu": q.n, "proteins": w["nproteins"],
+                       "index_entries": H.total_entries(), "index_ion_ids": H.total_ions(),
+                       "window_da": w["dM"], "frag_tol_bins": 5, "topK": 5,
+                       "l2": "inputs larger than L2 (index %.2f GB)" % (dev.nbytes / 1e9),
+                       "parallelism": f"replicas x{world}"},
+            "e2e": {"value": q.n * world / e2e_s, "unit": unit, "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "roofline": {"bound": "hbm", "kernel": top_k, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": bytes_launch, "kernel_ms": k_ms,
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback"},
+            "kernel_ms": {k: v[1] / v[0] for k, v in kt.items()},
+            "gpu_launches": launches,
+            "clocks": summarize_clocks(clocks),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,203 @@
+// Device-side building blocks of the query path shared by the search kernels.
+#pragma once
+
+#include <cstdint>
+
+#include "../../include/gicops_b200.h"
+
+namespace gx {
+
+constexpr int kHist = GX_HIST_BINS;
+constexpr int kMaxHeap = GX_MAX_HEAP;
+
+// Per-length constants of a device-resident index.
+struct DevLen {
+    uint64_t ia_off;      // first ion id of this length in the concatenated iA
+    uint64_t mass_off;    // first entry of this length in the concatenated masses
+    uint32_t npep;        // entries
+    uint32_t speclen;     // ions per entry
+    uint32_t half;        // speclen / 2 (b ions first, then y ions)
+    uint32_t peplen;
+};
+
+// Everything a search launch reads.
+struct SearchArgs {
+    // index
+    const uint32_t *bA;   // [nlen * nbins]
+    const uint32_t *iA;
+    const float *mass;
+    const DevLen *lens;
+    int32_t nlen;
+    uint32_t nbins;
+    uint32_t maxz;
+    // queries
+    const uint32_t *qidx;
+    const int32_t *moz;
+    const int32_t *intn;
+    const float *prec;
+    const double *dMq;
+    uint32_t nspec;
+    // parameters
+    double dM;
+    double upper;         // peaks need (double)m/z < upper = max_mass*scale - 1 - dF
+    uint32_t dF;
+    uint32_t min_shp;
+    uint32_t min_cpsm;
+    int32_t heap_cap;
+    double expect_max;
+    uint32_t flags;
+    const double *lgfact; // [81]
+    // scratch / outputs
+    const int2 *win;      // [nspec * nlen] candidate window per (spectrum, length)
+    gx_result *out;
+    gx_cell *heap_out;    // optional [nspec * heap_cap]
+    uint32_t *hist_out;   // optional [nspec * kHist]
+    int32_t *err;         // device guard word
+};
+
+// One heap cell as kept on chip.
+struct Cell {
+    float h;
+    int32_t psid;
+    uint16_t ixx;
+    uint16_t shp;
+    uint16_t total;
+    uint16_t pad;
+};
+
+// ---- minHeap<hCell> of the reference (source/core/include/minheap.h:103-271) ------
+__device__ __forceinline__ void heap_sift(Cell *a, int size, int i)
+{
+    for (;;) {
+        const int r = (i + 1) * 2, l = r - 1;
+        int s = i;
+        float sv = a[i].h;
+        if (l < size && a[l].h < sv) { s = l; sv = a[l].h; }
+        if (r < size && a[r].h < sv) { s = r; }
+        if (s == i) return;
+        const Cell t = a[s];
+        a[s] = a[i];
+        a[i] = t;
+        i = s;
+    }
+}
+
+__device__ __forceinline__ void heap_insert(Cell *a, int &size, int cap, const Cell &c)
+{
+    if (size == cap) {
+        if (c.h < a[0].h) return;
+        a[0] = c;
+        heap_sift(a, size, 0);
+        return;
+    }
+    a[size++] = c;
+    for (int i = (size - 1) / 2; i >= 0; i--) heap_sift(a, size, i);
+}
+
+__device__ __forceinline__ Cell heap_getmax(const Cell *a, int size)
+{
+    if (size <= 1) return a[0];
+    Cell m = a[size - 1];
+    for (int k = size - 2; k >= size / 2; k--)
+        if (a[k].h > m.h) m = a[k];
+    return m;
+}
+
+// double -> int with x86-64 cvttsd2si semantics (INT_MIN for NaN / out of range).
+__device__ __forceinline__ int32_t to_int_x86(double v)
+{
+    if (!(v > -2147483649.0 && v < 2147483648.0)) return (int32_t)0x80000000;
+    return (int32_t)v;
+}
+
+// expeRT::ModelTailFit (source/core/expeRT.cpp:396-559) followed by the e-value of
+// source/core/dslim_query.cpp:1017-1061.  Serial FP64 in one thread; the sums run in
+// the reference's order so the fit matches it.  `sx` is scratch for kHist+1 doubles.
+__device__ void tail_fit(const uint32_t *hist, int32_t cpsms, int32_t hyp, double *sx_buf, gx_result &r)
+{
+    double mu_t = 0.0, beta_t = 4.0;
+    int end1 = hyp - 1;
+    for (int p = hyp - 1; p >= 0; p--) if ((double)hist[p] >= 1.0) { end1 = p; break; }
+    int stt1 = 0;
+    for (int p = 0; p <= end1; p++) if ((double)hist[p] >= 1.0) { stt1 = p; break; }
+    if (stt1 == end1) end1 += 1;
+    if (cpsms < 1) {
+        mu_t = 0.0;
+        beta_t = 100.0;
+    } else {
+        sx_buf[0] = 0.0;  // the element before the slice (read when mark == -1)
+        double *sx = sx_buf + 1;
+        int size = end1 - stt1 + 1;
+        if (size < 0) size = 0;
+        double acc = 0.0;
+        for (int i = 0; i < size; i++) { acc = acc + (double)hist[stt1 + i]; sx[i] = acc; }
+        for (int i = 0; i < size; i++) {
+            double v = sx[i] / (double)cpsms;
+            v = v + (-1.0);
+            sx[i] = -v;
+            if (sx[i] > 1.0) sx[i] = 0.999;
+        }
+        if (size > 0) {
+            int rep = size - 1;
+            for (int p = size - 1; p >= 0; p--) if (sx[p] >= 1e-4) { rep = p; break; }
+            const double v = sx[rep];
+            for (int i = 0; i < size; i++) if (sx[i] <= 0.0) sx[i] = v;
+        }
+        for (int i = 0; i < size; i++) sx[i] = log10(sx[i]);
+        int mark = 0, mark2 = 0;
+        if (size >= 3) {
+            const double hgt = sx[size - 1] - sx[0];
+            const double t22 = sx[0] + hgt * 0.22;
+            int lm = 0;
+            for (int p = 0; p <= size - 1; p++) if (sx[p] <= t22) { lm = p; break; }
+            mark = lm - 1;
+            mark2 = size - 1;
+            if (size > 3) {
+                const double t87 = sx[0] + hgt * 0.87;
+                for (int p = size - 1; p >= 0; p--) if (sx[p] >= t87) { mark2 = p; break; }
+            }
+            if (mark >= mark2) mark = mark2 - 1;
+        } else {
+            mark = 0;
+            mark2 = size - 1;
+        }
+        const int n = mark2 - mark + 1;
+        if (n == 1) {
+            mu_t = 0.0;
+            beta_t = sx[mark];
+        } else if (n >= 2) {
+            double xbar = 0.0, ybar = 0.0;
+            for (int i = 0; i < n; i++) {
+                xbar = xbar + (double)(stt1 + mark + i);
+                ybar = ybar + sx[mark + i];
+            }
+            xbar = xbar / (double)n;
+            ybar = ybar / (double)n;
+            double top = 0.0, bot = 0.0;
+            for (int i = 0; i < n; i++) {
+                const double dx = (double)(stt1 + mark + i) - xbar;
+                top = top + dx * (sx[mark + i] - ybar);
+                bot = bot + dx * dx;
+            }
+            mu_t = top / bot;
+            beta_t = ybar - mu_t * xbar;
+        } else {
+            mu_t = __longlong_as_double(0x7ff8000000000000ll);
+            beta_t = mu_t;
+        }
+    }
+    r.slope = mu_t;
+    r.icpt = beta_t;
+    r.mu = to_int_x86(mu_t * 1e6);
+    r.beta = to_int_x86(beta_t * 1e6);
+    r.stt1 = stt1;
+    r.end1 = end1;
+    double w = (double)r.mu, b = (double)r.beta;
+    w /= 1e6;
+    b /= 1e6;
+    const double lgs = (w * (double)hyp) + b;
+    r.e_x = pow(10.0, lgs) * (double)(uint32_t)cpsms;
+    r.e_fp64 = pow(10.0, mu_t * (double)hyp + beta_t) * (double)(uint32_t)cpsms;
+}
+
+}  // namespace gx

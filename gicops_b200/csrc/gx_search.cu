@@ -1,0 +1,698 @@
+// Query path on sm_100a: precursor windows, fragment-ion bucket probes into a shared-
+// memory BYC scorecard, hyperscore + histogram + exact top-K heap, FP64 tail fit.
+//
+// Reference behaviour followed (paths relative to the reference project):
+//   source/core/dslim_query.cpp:749-1242 (DSLIM_QuerySpectrum, DSLIM_BinarySearch)
+//   source/core/expeRT.cpp:396-559, 1149-1289 (ModelTailFit, LinearFit)
+//   source/core/include/minheap.h:103-271 (top-K heap)
+// Compiled with -fmad=false: no multiply-add is fused, so every FP64 step rounds as
+// the reference's x86-64 build does.
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/gicops_b200.h"
+#include "gx_device.cuh"
+#include "gx_internal.h"
+
+namespace gx {
+
+namespace {
+thread_local std::string g_last_error;
+std::atomic<uint64_t> g_launches{0};
+}  // namespace
+
+gx_status fail(gx_status code, const std::string &msg)
+{
+    g_last_error = msg;
+    return code;
+}
+
+void count_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+// ---- opt-in kernel timing --------------------------------------------------------------
+namespace {
+struct ProfRec {
+    const char *name;
+    cudaEvent_t a, b;
+};
+std::mutex g_prof_mu;
+bool g_prof_on = false;
+std::vector<ProfRec> g_prof;
+}  // namespace
+
+// Records a start event on `st` when timing is on; returns a handle for prof_end.
+int prof_begin(const char *name, void *stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!g_prof_on) return -1;
+    ProfRec r{name, nullptr, nullptr};
+    if (cudaEventCreate(&r.a) != cudaSuccess || cudaEventCreate(&r.b) != cudaSuccess) return -1;
+    cudaEventRecord(r.a, st);
+    std::lock_guard<std::mutex> g(g_prof_mu);
+    g_prof.push_back(r);
+    return (int)g_prof.size() - 1;
+}
+
+void prof_end(int h, void *stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    if (h < 0) return;
+    std::lock_guard<std::mutex> g(g_prof_mu);
+    if (h < (int)g_prof.size()) cudaEventRecord(g_prof[h].b, st);
+}
+
+static gx_status cuda_fail(cudaError_t e, const char *what)
+{
+    return fail(GX_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define GX_CUDA(call)                                       \
+    do {                                                    \
+        cudaError_t e_ = (call);                            \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+    } while (0)
+
+// ------------------------------------------------------------------------------------
+// Kernels
+// ------------------------------------------------------------------------------------
+
+// Window [lo, hi] of every (spectrum, length): first entry with mass >= prec-dM, last
+// with mass <= prec+dM, both bounds rounded to float as the reference does
+// (dslim_query.cpp:1102-1164; its bisection helpers compute lower/upper bounds).
+__global__ void k_windows(SearchArgs a, int2 *win)
+{
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (uint64_t)a.nspec * a.nlen) return;
+    const uint32_t s = (uint32_t)(i / a.nlen);
+    const int l = (int)(i - (uint64_t)s * a.nlen);
+    const DevLen ln = a.lens[l];
+    const double dM = a.dMq ? a.dMq[s] : a.dM;
+    int lo = 1, hi = 0;
+    if (!(dM < 0.0) && ln.npep > 0) {
+        const float pr = a.prec[s];
+        const float p1 = __double2float_rn(__dsub_rn((double)pr, dM));
+        const float p2 = __double2float_rn(__dadd_rn((double)pr, dM));
+        const float *m = a.mass + ln.mass_off;
+        const uint32_t N = ln.npep;
+        if (p1 == p1 && p2 == p2 && !(p1 > m[N - 1]) && !(p2 < m[0])) {
+            uint32_t x = 0, y = N;
+            while (x < y) {
+                const uint32_t c = (x + y) >> 1;
+                if (m[c] < p1) x = c + 1; else y = c;
+            }
+            lo = (int)x;
+            x = 0;
+            y = N;
+            while (x < y) {
+                const uint32_t c = (x + y) >> 1;
+                if (p2 < m[c]) y = c; else x = c + 1;
+            }
+            hi = (int)x - 1;
+        }
+    }
+    win[i] = make_int2(lo, hi);
+}
+
+__device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t *__restrict__ v, uint32_t a, uint32_t b,
+                                                    uint32_t key)
+{
+    while (a < b) {
+        const uint32_t c = a + ((b - a) >> 1);
+        if (__ldg(v + c) < key) a = c + 1; else b = c;
+    }
+    return a;
+}
+
+constexpr int kBlock = 512;
+constexpr int kWarps = kBlock / 32;
+
+struct SearchSmem {
+    int32_t qmz[GX_MAX_PEAKS];
+    uint32_t qin[GX_MAX_PEAKS];
+    uint32_t hist[kHist];
+    double lgf[81];
+    Cell heap[kMaxHeap + 1];
+    Cell ent[kBlock];
+    int32_t warp_cnt[kWarps];
+    int32_t npk;
+    int32_t heap_size;
+    int32_t cpsms;
+    int32_t nent;
+    int32_t wide;
+    int32_t status;
+    float root;
+};
+
+// Scorecard words.  Packed (8 B per candidate): low word b ions, high word y ions,
+// each [count:8 | intensity sum:24]; valid while every per-candidate count stays
+// below 256 and every intensity sum below 2^24 (checked per spectrum).  Wide (12 B
+// per candidate): u32 counts (b low 16, y high 16), u32 b sum, u32 y sum, with the
+// reference's uint wrap-around.
+__device__ __forceinline__ void card_add_packed(unsigned long long *sc, uint32_t c, uint32_t isY, uint32_t in)
+{
+    const unsigned long long v = (unsigned long long)((1u << 24) | in) << (isY ? 32 : 0);
+    atomicAdd(sc + c, v);
+}
+
+// One spectrum per CTA.  Lengths run in index order, each window in tiles of
+// `tile` candidates; a tile is filled by probing every (peak, bin) bucket for the
+// ion ids whose entry falls in the tile, then scanned in entry order.
+__global__ void __launch_bounds__(kBlock) k_search_plain(SearchArgs a, int tile)
+{
+    extern __shared__ __align__(16) unsigned char dyn[];
+    __shared__ SearchSmem sm;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const uint32_t s = blockIdx.x;
+    if (s >= a.nspec) return;
+
+    // ---- peaks (only those the reference probes) -----------------------------------
+    if (tid == 0) {
+        sm.npk = 0;
+        sm.heap_size = 0;
+        sm.cpsms = 0;
+        sm.status = 0;
+        sm.root = 0.0f;
+    }
+    for (int i = tid; i < kHist; i += kBlock) sm.hist[i] = 0;
+    for (int i = tid; i < 81; i += kBlock) sm.lgf[i] = a.lgfact[i];
+    __syncthreads();
+    const uint32_t q0 = a.qidx[s], q1 = a.qidx[s + 1];
+    if (q1 - q0 > GX_MAX_PEAKS) {
+        if (tid == 0) atomicExch(a.err, 1);
+        return;
+    }
+    unsigned long long sum_in = 0;
+    for (uint32_t k = q0 + tid; k < q1; k += kBlock) {
+        const int32_t qi = a.moz[k];
+        if (qi > (int32_t)a.dF && (double)qi < a.upper) {
+            const int slot = atomicAdd(&sm.npk, 1);
+            sm.qmz[slot] = qi;
+            sm.qin[slot] = (uint32_t)a.intn[k];
+            sum_in += (uint32_t)a.intn[k];
+        }
+    }
+    // block sum of intensities for the packed-scorecard guard
+    for (int o = 16; o; o >>= 1) sum_in += __shfl_xor_sync(0xffffffffu, sum_in, o);
+    __shared__ unsigned long long wsum[kWarps];
+    if (lane == 0) wsum[wid] = sum_in;
+    __syncthreads();
+    if (tid == 0) {
+        unsigned long long t = 0;
+        for (int w = 0; w < kWarps; w++) t += wsum[w];
+        const bool ok = (uint64_t)sm.npk * a.maxz <= 255u && t * a.maxz < (1ull << 24);
+        sm.wide = (!ok || (a.flags & GX_FLAG_WIDE_SCORECARD)) ? 1 : 0;
+        if (sm.wide) sm.status |= 8;
+    }
+    __syncthreads();
+    // Peaks must be probed in any order: the scorecard sums are integer.
+    const int npk = sm.npk;
+    const bool wide = sm.wide != 0;
+    const int W = 2 * (int)a.dF + 1;
+    const int ctile = wide ? (tile * 2) / 3 : tile;
+    unsigned long long *scp = reinterpret_cast<unsigned long long *>(dyn);
+    uint32_t *scw_cnt = reinterpret_cast<uint32_t *>(dyn);
+    uint32_t *scw_ib = scw_cnt + ctile;
+    uint32_t *scw_iy = scw_ib + ctile;
+    for (int i = tid; i < (wide ? 3 * ctile : 2 * ctile); i += kBlock) reinterpret_cast<uint32_t *>(dyn)[i] = 0;
+    __syncthreads();
+
+    for (int ixx = 0; ixx < a.nlen; ixx++) {
+        const int2 w = a.win[(uint64_t)s * a.nlen + ixx];
+        if (w.y < w.x) continue;
+        const DevLen ln = a.lens[ixx];
+        const uint32_t *__restrict__ bA = a.bA + (uint64_t)ixx * a.nbins;
+        const uint32_t *__restrict__ iA = a.iA + ln.ia_off;
+        const uint32_t speclen = ln.speclen, half = ln.half;
+        for (int t0 = w.x; t0 <= w.y; t0 += ctile) {
+            const int t1 = min(w.y + 1, t0 + ctile);
+            const int tn = t1 - t0;
+            const uint32_t idlo = (uint32_t)t0 * speclen, idhi = (uint32_t)t1 * speclen;
+            // ---- probe buckets, scatter into the scorecard ----------------------------
+            for (int it = tid; it < npk * W; it += kBlock) {
+                const int k = it / W;
+                const uint32_t bin = (uint32_t)(sm.qmz[k] - (int32_t)a.dF + (it - k * W));
+                const uint32_t b0 = __ldg(bA + bin), b1 = __ldg(bA + bin + 1);
+                if (b1 <= b0) continue;
+                const uint32_t x = lower_bound_u32(iA, b0, b1, idlo);
+                const uint32_t y = lower_bound_u32(iA, x, b1, idhi);
+                const uint32_t in = sm.qin[k];
+                for (uint32_t ion = x; ion < y; ion++) {
+                    const uint32_t raw = __ldg(iA + ion);
+                    const uint32_t pp = raw / speclen;
+                    const uint32_t isY = (raw - pp * speclen) >= half ? 1u : 0u;
+                    const uint32_t c = pp - (uint32_t)t0;
+                    if (!wide) {
+                        card_add_packed(scp, c, isY, in);
+                    } else {
+                        atomicAdd(scw_cnt + c, isY ? 0x10000u : 1u);
+                        atomicAdd((isY ? scw_iy : scw_ib) + c, in);
+                    }
+                }
+            }
+            __syncthreads();
+            // ---- scan the tile in entry order ---------------------------------------
+            for (int c0 = 0; c0 < tn; c0 += kBlock) {
+                const int c = c0 + tid;
+                bool psm = false;
+                Cell cell;
+                if (c < tn) {
+                    uint32_t bc, yc, ib, iy;
+                    if (!wide) {
+                        const unsigned long long v = scp[c];
+                        const uint32_t lo = (uint32_t)v, hi = (uint32_t)(v >> 32);
+                        bc = lo >> 24; ib = lo & 0xFFFFFFu; yc = hi >> 24; iy = hi & 0xFFFFFFu;
+                        scp[c] = 0ull;
+                    } else {
+                        const uint32_t cnt = scw_cnt[c];
+                        bc = cnt & 0xFFFFu; yc = cnt >> 16; ib = scw_ib[c]; iy = scw_iy[c];
+                        scw_cnt[c] = 0; scw_ib[c] = 0; scw_iy[c] = 0;
+                    }
+                    const uint32_t shpk = (bc + yc) & 0xFFFFu;
+                    if (shpk >= a.min_shp) {
+                        uint32_t bi = bc, yi = yc;
+                        if (bi > 80u || yi > 80u) {
+                            atomicOr(&sm.status, 4);
+                            bi = min(bi, 80u);
+                            yi = min(yi, 80u);
+                        }
+                        const double h1 = sm.lgf[bi] + sm.lgf[yi];
+                        float h = __double2float_rn(h1 + log10((double)(uint32_t)(1u + ib)) +
+                                                    log10((double)(uint32_t)(1u + iy)) - 4.0);
+                        if (h > 0.0f) {
+                            if (h >= 80.0f) h = 79.0f;
+                            psm = true;
+                            cell.h = h;
+                            cell.psid = t0 + c;
+                            cell.ixx = (uint16_t)ixx;
+                            cell.shp = (uint16_t)shpk;
+                            cell.total = (uint16_t)speclen;
+                            cell.pad = 0;
+                            const int hb = __double2int_rz(__dadd_rn((double)__fmul_rn(h, 10.0f), 0.5));
+                            atomicAdd(&sm.hist[hb], 1u);
+                        }
+                    }
+                }
+                // entrants of the exact heap: every PSM while it is not full, else h >= root
+                const bool ent = psm && (sm.heap_size < a.heap_cap || cell.h >= sm.root);
+                const unsigned bal = __ballot_sync(0xffffffffu, ent);
+                const unsigned pbal = __ballot_sync(0xffffffffu, psm);
+                if (lane == 0) sm.warp_cnt[wid] = __popc(bal);
+                if (lane == 0 && pbal) atomicAdd(&sm.cpsms, __popc(pbal));
+                __syncthreads();
+                if (ent) {
+                    int base = 0;
+                    for (int w2 = 0; w2 < wid; w2++) base += sm.warp_cnt[w2];
+                    sm.ent[base + __popc(bal & ((1u << lane) - 1u))] = cell;
+                }
+                __syncthreads();
+                if (tid == 0) {
+                    int ne = 0;
+                    for (int w2 = 0; w2 < kWarps; w2++) ne += sm.warp_cnt[w2];
+                    int hs = sm.heap_size;
+                    for (int e = 0; e < ne; e++) heap_insert(sm.heap, hs, a.heap_cap, sm.ent[e]);
+                    sm.heap_size = hs;
+                    sm.root = sm.heap[0].h;
+                }
+                __syncthreads();
+            }
+        }
+    }
+
+    // ---- epilogue: top PSM, tail fit, outputs -----------------------------------------
+    if (a.hist_out)
+        for (int i = tid; i < kHist; i += kBlock) a.hist_out[(uint64_t)s * kHist + i] = sm.hist[i];
+    if (a.heap_out)
+        for (int i = tid; i < a.heap_cap; i += kBlock) {
+            gx_cell o{};
+            if (i < sm.heap_size) {
+                const Cell c = sm.heap[i];
+                o.hyperscore = c.h; o.psid = c.psid; o.idxoffset = c.ixx; o.sharedions = c.shp; o.totalions = c.total;
+            }
+            a.heap_out[(uint64_t)s * a.heap_cap + i] = o;
+        }
+    if (tid == 0) {
+        gx_result r;
+        memset(&r, 0, sizeof(r));
+        r.cpsms = sm.cpsms;
+        int st = sm.status;
+        if ((uint32_t)sm.cpsms >= a.min_cpsm) {
+            st |= 1;
+            const Cell t = heap_getmax(sm.heap, sm.heap_size);
+            r.top.hyperscore = t.h; r.top.psid = t.psid; r.top.idxoffset = t.ixx;
+            r.top.sharedions = t.shp; r.top.totalions = t.total;
+            r.maxhyp = __double2int_rz(__dadd_rn((double)__fmul_rn(t.h, 10.0f), 0.5));
+            tail_fit(sm.hist, sm.cpsms, r.maxhyp, reinterpret_cast<double *>(dyn), r);
+            if (r.e_x < a.expect_max) st |= 2;
+        }
+        r.status = st;
+        a.out[s] = r;
+    }
+}
+
+}  // namespace gx
+
+// ------------------------------------------------------------------------------------
+// Host API
+// ------------------------------------------------------------------------------------
+using namespace gx;
+
+struct gx_index {
+    int device = 0;
+    int32_t nlen = 0;
+    uint32_t nbins = 0;
+    uint32_t maxz = 0;
+    uint32_t *bA = nullptr;
+    uint32_t *iA = nullptr;
+    float *mass = nullptr;
+    DevLen *lens = nullptr;
+    std::vector<DevLen> hlens;
+    uint64_t bytes = 0;
+};
+
+namespace {
+constexpr int kDefaultTile = 8192;  // candidates per scorecard tile (8 B each)
+}
+
+struct gx_workspace {
+    const gx_index *ix = nullptr;
+    uint32_t max_spec = 0, max_peaks = 0;
+    int2 *win = nullptr;
+    double *lgfact = nullptr;
+    int32_t *err = nullptr;
+    // staging for gx_search_host
+    uint32_t *qidx = nullptr;
+    int32_t *moz = nullptr, *intn = nullptr, *charge = nullptr;
+    float *prec = nullptr;
+    double *dMq = nullptr;
+    gx_result *out = nullptr;
+    gx_cell *heap = nullptr;
+    uint32_t *hist = nullptr;
+    cudaStream_t stream = nullptr;
+};
+
+extern "C" const char *gx_last_error(void) { return g_last_error.c_str(); }
+
+extern "C" gx_status gx_profile_enable(int32_t on)
+{
+    std::lock_guard<std::mutex> g(g_prof_mu);
+    for (auto &r : g_prof) {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    g_prof.clear();
+    g_prof_on = on != 0;
+    return GX_SUCCESS;
+}
+
+extern "C" int32_t gx_profile_read(gx_kernel_time *out, int32_t cap)
+{
+    std::lock_guard<std::mutex> g(g_prof_mu);
+    std::vector<gx_kernel_time> agg;
+    for (auto &r : g_prof) {
+        float ms = 0.0f;
+        if (cudaEventSynchronize(r.b) != cudaSuccess || cudaEventElapsedTime(&ms, r.a, r.b) != cudaSuccess) continue;
+        gx_kernel_time *t = nullptr;
+        for (auto &x : agg)
+            if (std::strncmp(x.name, r.name, sizeof(x.name)) == 0) t = &x;
+        if (!t) {
+            agg.push_back(gx_kernel_time{});
+            t = &agg.back();
+            std::strncpy(t->name, r.name, sizeof(t->name) - 1);
+        }
+        t->launches += 1;
+        t->total_ms += ms;
+    }
+    const int n = (int)agg.size();
+    for (int i = 0; i < n && i < cap; i++) out[i] = agg[i];
+    return n;
+}
+extern "C" uint64_t gx_launch_count(void) { return g_launches.load(); }
+
+extern "C" void gx_lgfact(double *o)
+{
+    o[0] = o[1] = std::log10(1.0);
+    for (int i = 2; i < 81; i++) o[i] = std::log10((double)i) + o[i - 1];
+}
+
+extern "C" int32_t gx_heap_capacity(uint32_t topmatches)
+{
+    uint32_t num = topmatches == 0 ? 1 : topmatches;
+    num = (uint32_t)(std::floor(std::log2((double)num) + 0.999));
+    return (int32_t)((1u << num) - 1u);
+}
+
+extern "C" gx_status gx_index_upload(const gx_length_desc *lens, int32_t nlen, uint32_t nbins, int32_t device,
+                                     gx_index **out)
+{
+    if (!lens || !out) return fail(GX_ERR_INVLD_PTR, "gx_index_upload: null argument");
+    *out = nullptr;
+    if (nlen < 1 || nlen > GX_MAX_LENGTHS || nbins < 2)
+        return fail(GX_ERR_INVLD_PARAM, "gx_index_upload: nlen must be 1..64 and nbins >= 2");
+    uint32_t maxz = 0;
+    uint64_t tot_ia = 0, tot_m = 0;
+    std::vector<DevLen> hl(nlen);
+    for (int i = 0; i < nlen; i++) {
+        const gx_length_desc &d = lens[i];
+        if (d.peplen < 2 || d.speclen < 2 || d.speclen % (2 * (d.peplen - 1)) != 0)
+            return fail(GX_ERR_INVLD_INDEX, "gx_index_upload: speclen must be 2*(L-1)*maxz");
+        const uint32_t z = d.speclen / (2 * (d.peplen - 1));
+        if (maxz && z != maxz) return fail(GX_ERR_INVLD_INDEX, "gx_index_upload: lengths disagree on maxz");
+        maxz = z;
+        if ((uint64_t)d.npep * d.speclen >= (1ull << 32))
+            return fail(GX_ERR_INVLD_SIZE, "gx_index_upload: more than 2^32 ion ids in one length");
+        if (d.npep && (!d.mass || !d.bA || !d.iA)) return fail(GX_ERR_INVLD_PTR, "gx_index_upload: null array");
+        if (d.bA && d.bA[nbins - 1] != (uint64_t)d.npep * d.speclen)
+            return fail(GX_ERR_INVLD_INDEX, "gx_index_upload: bA[nbins-1] must equal npep*speclen");
+        hl[i] = DevLen{tot_ia, tot_m, d.npep, d.speclen, d.speclen / 2, d.peplen};
+        tot_ia += (uint64_t)d.npep * d.speclen;
+        tot_m += d.npep;
+    }
+    GX_CUDA(cudaSetDevice(device));
+    auto *ix = new gx_index();
+    ix->device = device;
+    ix->nlen = nlen;
+    ix->nbins = nbins;
+    ix->maxz = maxz;
+    ix->hlens = hl;
+    auto cleanup = [&](gx_status st) {
+        gx_index_free(ix);
+        return st;
+    };
+    cudaError_t e;
+    if ((e = cudaMalloc(&ix->bA, sizeof(uint32_t) * (uint64_t)nbins * nlen)) != cudaSuccess ||
+        (e = cudaMalloc(&ix->iA, sizeof(uint32_t) * (tot_ia ? tot_ia : 1))) != cudaSuccess ||
+        (e = cudaMalloc(&ix->mass, sizeof(float) * (tot_m ? tot_m : 1))) != cudaSuccess ||
+        (e = cudaMalloc(&ix->lens, sizeof(DevLen) * nlen)) != cudaSuccess) {
+        cudaGetLastError();
+        return cleanup(fail(GX_ERR_BAD_MEM_ALLOC, std::string("gx_index_upload: ") + cudaGetErrorString(e)));
+    }
+    ix->bytes = sizeof(uint32_t) * ((uint64_t)nbins * nlen + tot_ia) + sizeof(float) * tot_m + sizeof(DevLen) * nlen;
+    for (int i = 0; i < nlen; i++) {
+        const gx_length_desc &d = lens[i];
+        if ((e = cudaMemcpy(ix->bA + (uint64_t)i * nbins, d.bA, sizeof(uint32_t) * nbins, cudaMemcpyHostToDevice)) !=
+            cudaSuccess)
+            return cleanup(cuda_fail(e, "gx_index_upload bA"));
+        if (d.npep) {
+            if ((e = cudaMemcpy(ix->iA + hl[i].ia_off, d.iA, sizeof(uint32_t) * (uint64_t)d.npep * d.speclen,
+                                cudaMemcpyHostToDevice)) != cudaSuccess)
+                return cleanup(cuda_fail(e, "gx_index_upload iA"));
+            if ((e = cudaMemcpy(ix->mass + hl[i].mass_off, d.mass, sizeof(float) * d.npep, cudaMemcpyHostToDevice)) !=
+                cudaSuccess)
+                return cleanup(cuda_fail(e, "gx_index_upload mass"));
+        }
+    }
+    if ((e = cudaMemcpy(ix->lens, hl.data(), sizeof(DevLen) * nlen, cudaMemcpyHostToDevice)) != cudaSuccess)
+        return cleanup(cuda_fail(e, "gx_index_upload lens"));
+    *out = ix;
+    return GX_SUCCESS;
+}
+
+extern "C" gx_status gx_index_free(gx_index *ix)
+{
+    if (!ix) return GX_SUCCESS;
+    cudaSetDevice(ix->device);
+    cudaFree(ix->bA);
+    cudaFree(ix->iA);
+    cudaFree(ix->mass);
+    cudaFree(ix->lens);
+    delete ix;
+    return GX_SUCCESS;
+}
+
+extern "C" uint64_t gx_index_bytes(const gx_index *ix) { return ix ? ix->bytes : 0; }
+
+extern "C" gx_status gx_workspace_free(gx_workspace *ws)
+{
+    if (!ws) return GX_SUCCESS;
+    if (ws->ix) cudaSetDevice(ws->ix->device);
+    void *ptrs[] = {ws->win, ws->lgfact, ws->err, ws->qidx, ws->moz, ws->intn, ws->charge,
+                    ws->prec, ws->dMq, ws->out, ws->heap, ws->hist};
+    for (void *p : ptrs) cudaFree(p);
+    if (ws->stream) cudaStreamDestroy(ws->stream);
+    delete ws;
+    return GX_SUCCESS;
+}
+
+extern "C" gx_status gx_workspace_create(const gx_index *ix, uint32_t max_spec, uint32_t max_peaks,
+                                         gx_workspace **out)
+{
+    if (!ix || !out) return fail(GX_ERR_INVLD_PTR, "gx_workspace_create: null argument");
+    *out = nullptr;
+    if (max_spec == 0) return fail(GX_ERR_INVLD_PARAM, "gx_workspace_create: max_spec must be > 0");
+    GX_CUDA(cudaSetDevice(ix->device));
+    auto *ws = new gx_workspace();
+    ws->ix = ix;
+    ws->max_spec = max_spec;
+    ws->max_peaks = max_peaks;
+    cudaError_t e = cudaSuccess;
+    const uint64_t nw = (uint64_t)max_spec * ix->nlen;
+    auto al = [&](void **p, uint64_t bytes) {
+        if (e == cudaSuccess) e = cudaMalloc(p, bytes ? bytes : 16);
+    };
+    al((void **)&ws->win, sizeof(int2) * nw);
+    al((void **)&ws->lgfact, sizeof(double) * 81);
+    al((void **)&ws->err, sizeof(int32_t));
+    al((void **)&ws->qidx, sizeof(uint32_t) * (max_spec + 1));
+    al((void **)&ws->moz, sizeof(int32_t) * (uint64_t)max_peaks);
+    al((void **)&ws->intn, sizeof(int32_t) * (uint64_t)max_peaks);
+    al((void **)&ws->charge, sizeof(int32_t) * max_spec);
+    al((void **)&ws->prec, sizeof(float) * max_spec);
+    al((void **)&ws->dMq, sizeof(double) * max_spec);
+    al((void **)&ws->out, sizeof(gx_result) * max_spec);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        gx_workspace_free(ws);
+        return fail(GX_ERR_BAD_MEM_ALLOC, std::string("gx_workspace_create: ") + cudaGetErrorString(e));
+    }
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_search_plain, cudaFuncAttributeMaxDynamicSharedMemorySize, kDefaultTile * 8);
+    if (e != cudaSuccess) {
+        gx_workspace_free(ws);
+        return cuda_fail(e, "gx_workspace_create: kernel attributes");
+    }
+    double lg[81];
+    gx_lgfact(lg);
+    if ((e = cudaMemcpy(ws->lgfact, lg, sizeof(lg), cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemset(ws->err, 0, sizeof(int32_t))) != cudaSuccess) {
+        gx_workspace_free(ws);
+        return cuda_fail(e, "gx_workspace_create");
+    }
+    *out = ws;
+    return GX_SUCCESS;
+}
+
+namespace {
+
+gx_status check_params(const gx_index *ix, const gx_params *p, int32_t *cap)
+{
+    *cap = gx_heap_capacity(p->topmatches);
+    if (*cap < 1 || *cap > GX_MAX_HEAP)
+        return fail(GX_ERR_INVLD_PARAM, "topmatches gives a top-K heap capacity outside 1..31");
+    if (p->scale == 0 || p->dF > 255 || p->min_shp == 0)
+        return fail(GX_ERR_INVLD_PARAM, "scale must be > 0, dF <= 255, min_shp >= 1");
+    // bins probed: up to (max_mass*scale - 1 - dF) + dF + 1 must stay inside bA
+    const double top = p->max_mass * (double)p->scale;
+    if (!(top >= 1.0) || top + 1.0 > (double)ix->nbins + 0.5)
+        return fail(GX_ERR_INVLD_PARAM, "max_mass*scale+1 must not exceed the index's bins");
+    // the packed scorecard needs at most one ion per (charge, series) in a fragment window
+    if ((2.0 * p->dF + 1.0) * ix->maxz >= 57.02 * p->scale)
+        return fail(GX_ERR_INVLD_PARAM, "fragment tolerance wider than the smallest residue");
+    return GX_SUCCESS;
+}
+
+gx_status launch_search(gx_index *ix, gx_workspace *ws, const gx_queries *q, const gx_params *p, gx_result *out,
+                        gx_cell *heap, uint32_t *hist, cudaStream_t st)
+{
+    int32_t cap;
+    gx_status rc = check_params(ix, p, &cap);
+    if (rc != GX_SUCCESS) return rc;
+    if (q->nspec > ws->max_spec) return fail(GX_ERR_INVLD_SIZE, "more spectra than the workspace holds");
+    if (q->nspec == 0) return GX_SUCCESS;
+    SearchArgs a{};
+    a.bA = ix->bA; a.iA = ix->iA; a.mass = ix->mass; a.lens = ix->lens; a.nlen = ix->nlen; a.nbins = ix->nbins;
+    a.maxz = ix->maxz;
+    a.qidx = q->idx; a.moz = q->moz; a.intn = q->intn; a.prec = q->prec; a.dMq = q->dM; a.nspec = q->nspec;
+    a.dM = p->dM;
+    a.upper = (p->max_mass * (double)p->scale) - 1.0 - (double)p->dF;
+    a.dF = p->dF; a.min_shp = p->min_shp; a.min_cpsm = p->min_cpsm; a.heap_cap = cap;
+    a.expect_max = p->expect_max; a.flags = p->flags; a.lgfact = ws->lgfact;
+    a.win = ws->win; a.out = out; a.heap_out = heap; a.hist_out = hist; a.err = ws->err;
+
+    const uint64_t nw = (uint64_t)q->nspec * ix->nlen;
+    int h = prof_begin("k_windows", st);
+    k_windows<<<(unsigned)((nw + 255) / 256), 256, 0, st>>>(a, ws->win);
+    prof_end(h, st);
+    count_launch();
+    const int tile = kDefaultTile;
+    const size_t smem = (size_t)tile * 8;
+    h = prof_begin("k_search_plain", st);
+    k_search_plain<<<q->nspec, kBlock, smem, st>>>(a, tile);
+    prof_end(h, st);
+    count_launch();
+    GX_CUDA(cudaGetLastError());
+    return GX_SUCCESS;
+}
+
+}  // namespace
+
+extern "C" gx_status gx_search_device(gx_index *ix, gx_workspace *ws, const gx_queries *q, const gx_params *p,
+                                      gx_result *out, gx_cell *heap, uint32_t *hist, void *stream)
+{
+    if (!ix || !ws || !q || !p || !out) return fail(GX_ERR_INVLD_PTR, "gx_search_device: null argument");
+    if (ws->ix != ix) return fail(GX_ERR_INVLD_PARAM, "gx_search_device: workspace belongs to another index");
+    GX_CUDA(cudaSetDevice(ix->device));
+    return launch_search(ix, ws, q, p, out, heap, hist, (cudaStream_t)stream);
+}
+
+extern "C" gx_status gx_search_host(gx_index *ix, gx_workspace *ws, const gx_queries *q, const gx_params *p,
+                                    gx_result *out, gx_cell *heap_out, uint32_t *hist_out)
+{
+    if (!ix || !ws || !q || !p || !out) return fail(GX_ERR_INVLD_PTR, "gx_search_host: null argument");
+    if (ws->ix != ix) return fail(GX_ERR_INVLD_PARAM, "gx_search_host: workspace belongs to another index");
+    if (q->nspec > ws->max_spec || q->npeaks > ws->max_peaks)
+        return fail(GX_ERR_INVLD_SIZE, "gx_search_host: batch larger than the workspace");
+    if (q->nspec == 0) return GX_SUCCESS;
+    if (!q->idx || !q->moz || !q->intn || !q->prec) return fail(GX_ERR_INVLD_PTR, "gx_search_host: null query array");
+    if (q->idx[q->nspec] != q->npeaks) return fail(GX_ERR_INVLD_PARAM, "gx_search_host: idx[nspec] != npeaks");
+    int32_t cap;
+    gx_status rc = check_params(ix, p, &cap);
+    if (rc != GX_SUCCESS) return rc;
+    GX_CUDA(cudaSetDevice(ix->device));
+    cudaStream_t st = ws->stream;
+    const uint32_t n = q->nspec;
+    if (heap_out && !ws->heap) GX_CUDA(cudaMalloc(&ws->heap, sizeof(gx_cell) * GX_MAX_HEAP * (uint64_t)ws->max_spec));
+    if (hist_out && !ws->hist) GX_CUDA(cudaMalloc(&ws->hist, sizeof(uint32_t) * GX_HIST_BINS * (uint64_t)ws->max_spec));
+    GX_CUDA(cudaMemcpyAsync(ws->qidx, q->idx, sizeof(uint32_t) * (n + 1), cudaMemcpyHostToDevice, st));
+    GX_CUDA(cudaMemcpyAsync(ws->moz, q->moz, sizeof(int32_t) * q->npeaks, cudaMemcpyHostToDevice, st));
+    GX_CUDA(cudaMemcpyAsync(ws->intn, q->intn, sizeof(int32_t) * q->npeaks, cudaMemcpyHostToDevice, st));
+    GX_CUDA(cudaMemcpyAsync(ws->prec, q->prec, sizeof(float) * n, cudaMemcpyHostToDevice, st));
+    if (q->dM) GX_CUDA(cudaMemcpyAsync(ws->dMq, q->dM, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+    gx_queries dq = *q;
+    dq.idx = ws->qidx; dq.moz = ws->moz; dq.intn = ws->intn; dq.prec = ws->prec;
+    dq.charge = nullptr;
+    dq.dM = q->dM ? ws->dMq : nullptr;
+    rc = launch_search(ix, ws, &dq, p, ws->out, heap_out ? ws->heap : nullptr, hist_out ? ws->hist : nullptr, st);
+    if (rc != GX_SUCCESS) return rc;
+    GX_CUDA(cudaMemcpyAsync(out, ws->out, sizeof(gx_result) * n, cudaMemcpyDeviceToHost, st));
+    if (heap_out)
+        GX_CUDA(cudaMemcpyAsync(heap_out, ws->heap, sizeof(gx_cell) * cap * (uint64_t)n, cudaMemcpyDeviceToHost, st));
+    if (hist_out)
+        GX_CUDA(cudaMemcpyAsync(hist_out, ws->hist, sizeof(uint32_t) * GX_HIST_BINS * (uint64_t)n,
+                                cudaMemcpyDeviceToHost, st));
+    int32_t err = 0;
+    GX_CUDA(cudaMemcpyAsync(&err, ws->err, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    GX_CUDA(cudaStreamSynchronize(st));
+    if (err) {
+        cudaMemsetAsync(ws->err, 0, sizeof(int32_t), st);
+        return fail(GX_ERR_DEVICE_GUARD, "a spectrum has more peaks than GX_MAX_PEAKS");
+    }
+    return GX_SUCCESS;
+}

@@ -1,0 +1,216 @@
+/* gicops_b200: B200-native peptide-search query path (DSLIM fragment-ion index
+ * lookup -> BYC shared-peak scorecard -> hyperscore -> top-K -> score histogram ->
+ * tail-fit e-value) behind a plain C ABI.
+ *
+ * The entry points replace the reference's query-path boundary (paths are
+ * relative to the reference project, mhaseeb123/gicops):
+ *   hcp::gpu::cuda::s3::initialize / search / deinitialize / getBYC / getScorecard /
+ *   reset_dScores   source/core/include/cuda/superstep3/kernel.hpp:88-100
+ *   hcp::gpu::cuda::s1::getdIndex (index residency)   source/core/cuda/superstep1/kernel.cu:310-358
+ *   hcp::gpu::cuda::s4::processResults (tail fit + results) source/core/cuda/superstep4/kernel.cu:491-596
+ *   DSLIM_QuerySpectrum (CPU query path)           source/core/include/dslim.h:196
+ *   DSLIM_Construct + LBE_* (host index build)     source/core/dslim.cpp:46-153, source/core/lbe_internal.cpp
+ *
+ * Conventions: every call returns a gx_status (codes mirror source/core/include/slmerr.h)
+ * and never exits the process; gx_last_error() gives the message of the calling
+ * thread's last failure.  Calls are thread-compatible: use one gx_workspace per host
+ * thread.  Device-pointer calls are stream-ordered and do not synchronise.
+ */
+#ifndef GICOPS_B200_H
+#define GICOPS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (source/core/include/slmerr.h:24-43) ------------------------------ */
+typedef int32_t gx_status;
+#define GX_SUCCESS             0
+#define GX_ERR_INVLD_MEMORY    (-3001)
+#define GX_ERR_INVLD_PARAM     (-3002)
+#define GX_ERR_INVLD_INDEX     (-3003)
+#define GX_ERR_INVLD_SIZE      (-3004)
+#define GX_ERR_BAD_MEM_ALLOC   (-3007)
+#define GX_ERR_INVLD_PTR       (-3008)
+#define GX_ERR_INVLD_MOD       (-3010)
+#define GX_ERR_NOT_ENOUGH_DATA (-3012)
+/* additions (no counterpart in slmerr.h): CUDA failure, device-side guard tripped */
+#define GX_ERR_CUDA            (-3050)
+#define GX_ERR_DEVICE_GUARD    (-3051)
+
+#define GX_HIST_BINS 802      /* 2 + MAX_HYPERSCORE*10 (source/core/include/expeRT.h:115) */
+#define GX_MAX_HEAP  31       /* largest top-K heap capacity supported (topmatches <= 31) */
+#define GX_MAX_LENGTHS 64     /* peptide lengths per index */
+#define GX_MAX_PEAKS 1024     /* peaks per spectrum (the reference's QALEN is 100) */
+
+/* ---- index (source/core/include/slm_dsts.h:146-346) --------------------------------- */
+
+/* One index entry (pepEntry, slm_dsts.h:146): precursor mass, sequence id within its
+ * length, modification site mask, modification numbers (4 bits per modified site). */
+typedef struct {
+    float mass;
+    uint32_t seqid;
+    uint64_t sites;
+    uint32_t modnum;
+    uint32_t pad;
+} gx_pep_entry;
+
+/* Query-path view of one per-length index (Index + its single ionIndex chunk). */
+typedef struct {
+    uint32_t peplen;      /* L */
+    uint32_t npep;        /* N entries (peptides + variants), ascending mass */
+    uint32_t speclen;     /* ions per entry = 2*(L-1)*maxz */
+    uint32_t pad;
+    const float *mass;    /* [N] entry masses, ascending */
+    const uint32_t *bA;   /* [nbins] CSR offsets per 0.01 Da fragment bin (DSLIM_Matrix.bA) */
+    const uint32_t *iA;   /* [N*speclen] ion ids pepid*speclen+pos, ascending in a bin (DSLIM_Matrix.iA) */
+} gx_length_desc;
+
+typedef struct gx_index gx_index;          /* device-resident index (opaque) */
+typedef struct gx_workspace gx_workspace;  /* device scratch for one host thread (opaque) */
+
+/* Upload (copy) the per-length host arrays into HBM on `device`; replaces
+ * s1::getdIndex.  nbins must be max_mass*scale + 1.  Lengths must be given in the
+ * order their results are to be reported (idxoffset = position in this array). */
+gx_status gx_index_upload(const gx_length_desc *lens, int32_t nlen, uint32_t nbins, int32_t device,
+                          gx_index **out);
+gx_status gx_index_free(gx_index *ix);
+/* bytes held in HBM by an index */
+uint64_t gx_index_bytes(const gx_index *ix);
+
+/* ---- host index builder (LBE_CountPeps/Initialize + MODS_GenerateMods + DSLIM_Construct) */
+typedef struct {
+    char residues[4];     /* residues the modification applies to, NUL padded */
+    double mass;          /* Da; stored as (uint)(mass*scale) like argp.hpp:359 */
+    uint32_t max_per_pep; /* per-peptide limit for this modification */
+} gx_mod;
+
+typedef struct {
+    uint32_t maxz;        /* fragment charges indexed */
+    uint32_t scale;       /* bins per Da (100) */
+    uint32_t min_mass, max_mass;   /* precursor mass filter (500, 5000) */
+    uint32_t nmods;       /* number of gx_mod entries */
+    uint32_t mods_per_pep;/* total modified residues per peptide (0: no variants) */
+    const gx_mod *mods;
+    int32_t threads;      /* host threads (<=0: all) */
+} gx_build_params;
+
+typedef struct gx_host_length gx_host_length;  /* host-side per-length index (opaque) */
+
+/* Build the index of one peptide length from `npep` sequences of length L
+ * (row-major, no separators, the order of the L.peps file). */
+gx_status gx_build_length(const char *seqs, uint32_t npep, uint32_t L, const gx_build_params *bp,
+                          gx_host_length **out);
+/* Accessors: the descriptor points into the object; entries, kept sequences
+ * (peptides that passed the mass filter, index seqid order). */
+gx_status gx_host_length_desc(const gx_host_length *h, gx_length_desc *desc);
+const gx_pep_entry *gx_host_length_entries(const gx_host_length *h);
+const char *gx_host_length_seqs(const gx_host_length *h, uint32_t *npep_kept);
+void gx_host_length_free(gx_host_length *h);
+
+/* ---- search ------------------------------------------------------------------------ */
+typedef struct {
+    double dM;            /* precursor tolerance (Da), used when gx_queries.dM is NULL */
+    uint32_t dF;          /* fragment tolerance (bins) */
+    uint32_t scale;       /* bins per Da */
+    double max_mass;      /* Da */
+    uint32_t min_shp;     /* shared peaks for a candidate PSM (4) */
+    uint32_t min_cpsm;    /* candidate PSMs for an e-value (4) */
+    uint32_t topmatches;  /* heap capacity = 2^floor(log2(t)+0.999) - 1 (dslim.cpp:438-444) */
+    uint32_t flags;       /* GX_FLAG_* */
+    double expect_max;    /* PSMs with e >= expect_max are not reported */
+} gx_params;
+
+#define GX_FLAG_WIDE_SCORECARD 1u   /* force the 12-byte scorecard (testing) */
+#define GX_FLAG_PLAIN          2u   /* one spectrum per CTA, no work queue (plain path) */
+
+/* Spectra in the reference's Queries<int> layout (slm_dsts.h:520-658). */
+typedef struct {
+    uint32_t nspec;
+    uint32_t npeaks;      /* idx[nspec] */
+    const uint32_t *idx;  /* [nspec+1] */
+    const int32_t *moz;   /* [npeaks] m/z bins */
+    const int32_t *intn;  /* [npeaks] intensities */
+    const float *prec;    /* [nspec] precursor masses */
+    const int32_t *charge;/* [nspec] (reported only) */
+    const double *dM;     /* [nspec] per-spectrum tolerance (Da) or NULL */
+} gx_queries;
+
+/* One candidate PSM (hCell's query-path fields, slm_dsts.h:661-761). */
+typedef struct {
+    float hyperscore;
+    int32_t psid;         /* entry index within its length */
+    uint16_t idxoffset;   /* length index */
+    uint16_t sharedions;
+    uint16_t totalions;
+    uint16_t pad;
+} gx_cell;
+
+/* Per-spectrum result.  status bits: 1 = cpsms >= min_cpsm (e-value computed),
+ * 2 = e_x < expect_max (a PSM the reference prints), 4 = a shared-ion count above
+ * MAX_SHDPEAKS (80) was clamped, 8 = the 12-byte scorecard was used. */
+typedef struct {
+    int32_t cpsms;
+    int32_t status;
+    gx_cell top;          /* minHeap::getMax() of the reference's top-K heap */
+    int32_t maxhyp;       /* (int)(top.hyperscore*10+0.5) */
+    int32_t mu, beta;     /* tail-fit slope/intercept x1e6 truncated (Results.mu/beta) */
+    int32_t stt1, end1;   /* tail-fit curve region */
+    int32_t pad;
+    double slope, icpt;   /* unquantized FP64 fit */
+    double e_x;           /* e-value as the reference computes it */
+    double e_fp64;        /* e-value from the unquantized fit */
+} gx_result;
+
+/* Workspace sized for up to max_spec spectra / max_peaks peaks per call. */
+gx_status gx_workspace_create(const gx_index *ix, uint32_t max_spec, uint32_t max_peaks, gx_workspace **out);
+gx_status gx_workspace_free(gx_workspace *ws);
+
+/* Search with HOST buffers (the drop-in for s3::search + s4::processResults):
+ * copies queries in, runs the path, copies results out, synchronises.
+ * heap_out (optional): [nspec * cap] final heap arrays; hist_out (optional):
+ * [nspec * GX_HIST_BINS] score histograms. */
+gx_status gx_search_host(gx_index *ix, gx_workspace *ws, const gx_queries *q, const gx_params *p,
+                         gx_result *out, gx_cell *heap_out, uint32_t *hist_out);
+
+/* Search with DEVICE buffers already resident in HBM (stream-ordered, no sync). */
+gx_status gx_search_device(gx_index *ix, gx_workspace *ws, const gx_queries *q_dev, const gx_params *p,
+                           gx_result *out_dev, gx_cell *heap_dev, uint32_t *hist_dev, void *stream);
+
+/* Algorithmic traffic of the path, per spectrum (host arrays, for roofline figures):
+ * ids_out[s] = ion ids inside the precursor window of every distinct probed bin,
+ * bins_out[s] = distinct probed bins, both summed over lengths with a non-empty
+ * window.  No counterpart in the reference (measurement only). */
+gx_status gx_traffic_host(const gx_length_desc *lens, int32_t nlen, const gx_queries *q, const gx_params *p,
+                          int64_t *ids_out, int64_t *bins_out, int32_t threads);
+
+/* Heap capacity the reference uses for `topmatches` (dslim.cpp:438-444). */
+int32_t gx_heap_capacity(uint32_t topmatches);
+
+/* Hyperscore table: out[i] = sum_{k<=i} log10(k), i = 0..80 (utils.h:115-131). */
+void gx_lgfact(double *out81);
+
+/* Kernel timing: when enabled, every kernel the library launches is bracketed by
+ * CUDA events recorded on its own stream.  gx_profile_read synchronises those
+ * events and returns per-kernel totals (launches, milliseconds); enabling again
+ * clears them.  No counterpart in the reference (it times with host clocks). */
+typedef struct {
+    char name[40];
+    uint64_t launches;
+    double total_ms;
+} gx_kernel_time;
+gx_status gx_profile_enable(int32_t on);
+int32_t gx_profile_read(gx_kernel_time *out, int32_t cap);
+
+/* Message of the calling thread's last failure ("" if none). */
+const char *gx_last_error(void);
+/* Kernel launches issued by this process so far (all gx_* calls). */
+uint64_t gx_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GICOPS_B200_H */

@@ -1,0 +1,153 @@
+"""GPU query path vs the oracle and vs the reference's captured PSMs.
+
+Bit-exact: candidate counts, histogram bins, top-K heap contents (ids, shared ions,
+float hyperscores), the reported top PSM, tail-fit region and the quantized
+slope/intercept (mu, beta).  Floating point: e-values within 1e-9 relative (the
+only differences allowed come from the device's log10/pow, which may differ from
+the host C library in the last bit).
+"""
+
+import numpy as np
+import pytest
+
+import pyoracle
+from conftest import CASES, has_gpu, oracle_params, search_params
+
+pytestmark = pytest.mark.gpu
+
+E_RTOL = 1e-9
+
+
+@pytest.fixture(scope="module")
+def gx():
+    if not has_gpu():
+        pytest.skip("no CUDA device")
+    import gicops_b200
+    return gicops_b200
+
+
+def _heap_cells(arr):
+    return [(float(c["hyperscore"]), int(c["psid"]), int(c["idxoffset"]), int(c["sharedions"]), int(c["totalions"]))
+            for c in arr]
+
+
+def assert_same(res, heap, hist, ores, ohist, cap):
+    assert np.array_equal(res["cpsms"], ores["cpsms"])
+    assert np.array_equal(res["status"] & 7, ores["status"] & 7)
+    assert np.array_equal(hist, ohist)
+    for i in range(len(res)):
+        n = int(ores["heap_size"][i])
+        assert _heap_cells(heap[i][:n]) == _heap_cells(ores["heap"][i][:n]), i
+        assert np.all(heap[i][n:]["psid"] == 0)
+    m = (ores["status"] & 1) != 0
+    for f in ("psid", "idxoffset", "sharedions", "totalions"):
+        assert np.array_equal(res["top"][f][m], ores["top"][f][m]), f
+    assert np.array_equal(res["top"]["hyperscore"][m].view(np.uint32), ores["top"]["hyperscore"][m].view(np.uint32))
+    for f in ("maxhyp", "mu", "beta", "stt1", "end1"):
+        assert np.array_equal(res[f][m], ores[f][m]), f
+    ok = m & np.isfinite(ores["e_x"])
+    np.testing.assert_allclose(res["e_x"][ok], ores["e_x"][ok], rtol=E_RTOL)
+    np.testing.assert_allclose(res["slope"][ok], ores["slope"][ok], rtol=1e-12, atol=1e-15)
+    np.testing.assert_allclose(res["e_fp64"][ok], ores["e_fp64"][ok], rtol=E_RTOL)
+    if cap is not None:
+        rep = (res["status"] & 2) != 0
+        assert np.array_equal(rep, cap["cap_reported"] == 1)
+        assert np.array_equal(res["top"]["psid"][rep], cap["cap_psid"][rep])
+        assert np.array_equal(res["top"]["idxoffset"][rep], cap["cap_idxoffset"][rep])
+        assert np.array_equal(res["top"]["hyperscore"][rep].view(np.uint32), cap["cap_hyperscore"][rep].view(np.uint32))
+        np.testing.assert_allclose(res["e_x"][rep], cap["cap_e_x"][rep], rtol=E_RTOL)
+
+
+@pytest.mark.parametrize("case", CASES)
+@pytest.mark.parametrize("flags", [0, 1, 2], ids=["default", "wide", "plain"])
+def test_gpu_golden(gx, golden, case, flags):
+    c = golden(case)
+    H, q = c["index"], c["queries"]
+    dev = gx.DeviceIndex(H, 0)
+    s = gx.Searcher(dev, q.n, len(q.moz))
+    r = s.search(q, search_params(c, flags=flags), heap=True, hist=True)
+    ores, ohist = pyoracle.search(H.lengths, q, oracle_params(c), hist=True)
+    assert_same(r.result, r.heap, r.hist, ores, ohist, c)
+    if flags == 1:
+        assert np.all((r.result["status"] & 8) != 0)
+
+
+def test_gpu_without_optional_outputs(gx, golden):
+    c = golden("open_mox")
+    dev = gx.DeviceIndex(c["index"], 0)
+    s = gx.Searcher(dev, c["queries"].n, len(c["queries"].moz))
+    a = s.search(c["queries"], search_params(c))
+    b = s.search(c["queries"], search_params(c), heap=True, hist=True)
+    assert a.heap is None and a.hist is None
+    assert a.result.tobytes() == b.result.tobytes()
+
+
+@pytest.mark.parametrize("seed", [21, 22])
+def test_gpu_random_open_search(gx, seed):
+    """Seeded open search (+-500 Da, Met-ox, charge-2 fragments) beyond the fixtures."""
+    db = gx.synth.make_database(600, seed=seed)
+    H = gx.HostIndex.build(db, maxz=2, mods=[("M", 15.9949, 2)], nmods=2)
+    q = gx.synth.make_queries(H.entries_by_len(), 300, seed=seed + 1, charges=(2, 4), frag_charge2=True,
+                              keep_p=(0.2, 0.8), noise_mode="fill")
+    p = gx.SearchParams(dM=500.0, expect_max=1e300)
+    dev = gx.DeviceIndex(H, 0)
+    s = gx.Searcher(dev, q.n, len(q.moz))
+    r = s.search(q, p, heap=True, hist=True)
+    ores, ohist = pyoracle.search(H.lengths, q, pyoracle.Params(dM=500.0), hist=True)
+    assert_same(r.result, r.heap, r.hist, ores, ohist, None)
+
+
+def test_gpu_topmatches_and_min_shp(gx, golden):
+    """Other heap capacities (topmatches 10 -> 15 cells) and shared-peak thresholds."""
+    c = golden("open_mox")
+    H, q = c["index"], c["queries"]
+    dev = gx.DeviceIndex(H, 0)
+    s = gx.Searcher(dev, q.n, len(q.moz))
+    for tm, shp in [(10, 4), (2, 3), (31, 6)]:
+        p = gx.SearchParams(dM=500.0, topmatches=tm, min_shp=shp, expect_max=1e300)
+        r = s.search(q, p, heap=True, hist=True)
+        ores, ohist = pyoracle.search(H.lengths, q, pyoracle.Params(dM=500.0, topmatches=tm, min_shp=shp), hist=True)
+        assert_same(r.result, r.heap, r.hist, ores, ohist, None)
+
+
+def test_gpu_empty_and_degenerate_spectra(gx, golden):
+    c = golden("closed_small")
+    H = c["index"]
+    q = gx.synth.QueryBatch(
+        idx=np.array([0, 0, 3, 4, 6], np.uint32),
+        moz=np.array([3, 499999, -7, 150000, 100000, 100000], np.int32),   # filtered peaks, one peak, duplicates
+        intn=np.array([100, 100, 100, 100000, 5000, 5000], np.int32),
+        prec=np.array([1500.0, 1500.0, 100.0, 1200.0], np.float32),
+        charge=np.array([2, 2, 2, 2], np.int32), rtime=np.zeros(4, np.float32))
+    dev = gx.DeviceIndex(H, 0)
+    s = gx.Searcher(dev, 8, 64)
+    p = search_params(c)
+    r = s.search(q, p, heap=True, hist=True)
+    ores, ohist = pyoracle.search(H.lengths, q, oracle_params(c), hist=True)
+    assert_same(r.result, r.heap, r.hist, ores, ohist, None)
+    # an empty batch is a no-op
+    e = gx.synth.QueryBatch(np.zeros(1, np.uint32), np.zeros(0, np.int32), np.zeros(0, np.int32),
+                            np.zeros(0, np.float32), np.zeros(0, np.int32), np.zeros(0, np.float32))
+    assert s.search(e, p).result.shape == (0,)
+
+
+def test_gpu_errors_are_status_codes(gx, golden):
+    c = golden("closed_small")
+    H, q = c["index"], c["queries"]
+    dev = gx.DeviceIndex(H, 0)
+    s = gx.Searcher(dev, 4, 4096)
+    with pytest.raises(gx.GxError) as e:
+        s.search(q, search_params(c))                      # more spectra than the workspace
+    assert e.value.code == -3004
+    with pytest.raises(gx.GxError) as e:
+        s.search(q.subset([0]), gx.SearchParams(topmatches=1))   # zero-capacity heap
+    assert e.value.code == -3002
+    big = gx.synth.QueryBatch(np.array([0, 2000], np.uint32), np.full(2000, 100000, np.int32),
+                              np.full(2000, 1000, np.int32), np.array([1500.0], np.float32),
+                              np.array([2], np.int32), np.zeros(1, np.float32))
+    with pytest.raises(gx.GxError) as e:
+        s.search(big, search_params(c))                   # more peaks than a CTA holds
+    assert e.value.code == -3051
+    # the context stays usable afterwards
+    r = s.search(q.subset([0, 1]), search_params(c))
+    assert r.result.shape == (2,)
