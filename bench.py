@@ -140,6 +140,8 @@ def main():
     ap.add_argument("--workload", default="open-20k", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plain", action="store_true", help="time the plain one-spectrum-per-CTA path instead")
+    ap.add_argument("--compare-plain", action="store_true", help="also time one step of the plain path")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -178,7 +180,8 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
 
     w, db, H, q = make_workload(args.workload, rank)
-    params = gx.SearchParams(dM=w["dM"], dF=5, topmatches=5, expect_max=20.0)
+    params = gx.SearchParams(dM=w["dM"], dF=5, topmatches=5, expect_max=20.0,
+                             flags=gx.FLAG_PLAIN if args.plain else 0)
     dev = gx.DeviceIndex(H, local)
     ws = gx.Searcher(dev, q.n, len(q.moz))
     stream = torch.cuda.current_stream()
@@ -278,6 +281,18 @@ def main():
         if ent:
             traffic = ent["dram_bytes_per_launch"]
 
+    plain = None
+    if args.compare_plain and not args.plain:
+        import dataclasses
+        pp = dataclasses.replace(params, flags=gx.FLAG_PLAIN)
+        ws.search_device(qd, pp, t_out.data_ptr(), stream=stream.cuda_stream)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        ws.search_device(qd, pp, t_out.data_ptr(), stream=stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        plain = {"value": q.n / (e0.elapsed_time(e1) / 1e3), "unit": unit, "steps": 1}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -306,6 +321,8 @@ def main():
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback"},
             "kernel_ms": {k: v[1] / v[0] for k, v in kt.items()},
             "gpu_launches": launches,
+            "path": "plain" if args.plain else "batched",
+            "plain_path": plain,
             "clocks": summarize_clocks(clocks),
             "cpu_baseline": cpu,
         }

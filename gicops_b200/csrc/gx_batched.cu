@@ -1,0 +1,612 @@
+// Batched query path: one persistent kernel fed by a work queue of spectra sorted by
+// their scan volume, heaviest first.
+//
+//   k_prep          per spectrum: precursor windows of every length, the peak windows
+//                   merged into disjoint bin intervals (coverage count, intensity sum),
+//                   the packed-scorecard guard and the scan volume (sort key)
+//   (radix sort of the spectra by scan volume, descending)
+//   k_search_batched  persistent CTAs; per spectrum, per length, per candidate tile:
+//                   stream the iA span of every interval (each bucket read once),
+//                   accumulate the BYC scorecard in shared memory, then scan the tile
+//                   in entry order (hyperscore, histogram, exact top-K heap)
+//   k_tailfit       one warp per spectrum: expeRT tail fit and e-value
+//
+// Results are identical to the reference's CPU path (source/core/dslim_query.cpp:
+// 827-1061): every (peak, bin, ion) match of the reference is counted once per
+// covering peak, through the interval's coverage count and intensity sum.
+
+#include <cub/cub.cuh>
+#include <cuda_runtime.h>
+
+#include "../../include/gicops_b200.h"
+#include "gx_batched.h"
+#include "gx_device.cuh"
+#include "gx_internal.h"
+
+namespace gx {
+
+// ------------------------------------------------------------------------------------
+// k_prep: one CTA per spectrum
+// ------------------------------------------------------------------------------------
+constexpr int kPrepBlock = 256;
+
+__global__ void __launch_bounds__(kPrepBlock) k_prep(SearchArgs a, int2 *win, uint64_t *work_key, uint32_t *order0)
+{
+    __shared__ int32_t pk[GX_MAX_PEAKS];
+    __shared__ uint32_t pi[GX_MAX_PEAKS];
+    __shared__ int32_t npk_s;
+    __shared__ unsigned long long red[kPrepBlock / 32];
+    __shared__ uint32_t nv_s;
+    const int tid = threadIdx.x;
+    const uint32_t s = blockIdx.x;
+    if (s >= a.nspec) return;
+    const uint32_t q0 = a.qidx[s], q1 = a.qidx[s + 1];
+    if (tid == 0) npk_s = 0;
+    __syncthreads();
+    if (q1 < q0 || q1 - q0 > GX_MAX_PEAKS || 2ull * q1 > a.ivl_cap) {
+        if (tid == 0) {
+            atomicExch(a.err, 1);
+            a.nivl[s] = 0;
+            a.guard[s] = 1;
+            work_key[s] = 0;
+            order0[s] = s;
+        }
+        for (int l = tid; l < a.nlen; l += kPrepBlock) win[(uint64_t)s * a.nlen + l] = make_int2(1, 0);
+        return;
+    }
+    // valid peaks (those the reference probes), padded to a power of two for the sort
+    unsigned long long isum = 0;
+    for (uint32_t k = q0 + tid; k < q1; k += kPrepBlock) {
+        const int32_t m = a.moz[k];
+        if (m > (int32_t)a.dF && (double)m < a.upper) {
+            const int slot = atomicAdd(&npk_s, 1);
+            pk[slot] = m;
+            pi[slot] = (uint32_t)a.intn[k];
+            isum += (uint32_t)a.intn[k];
+        }
+    }
+    __syncthreads();
+    const int n = npk_s;
+    int np2 = 1;
+    while (np2 < n) np2 <<= 1;
+    for (int i = n + tid; i < np2; i += kPrepBlock) {
+        pk[i] = 0x7fffffff;
+        pi[i] = 0;
+    }
+    __syncthreads();
+    // bitonic sort of (m/z, intensity) by m/z
+    for (int k = 2; k <= np2; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = tid; i < np2; i += kPrepBlock) {
+                const int l = i ^ j;
+                if (l > i) {
+                    const bool up = (i & k) == 0;
+                    if ((pk[i] > pk[l]) == up) {
+                        const int32_t t = pk[i]; pk[i] = pk[l]; pk[l] = t;
+                        const uint32_t u = pi[i]; pi[i] = pi[l]; pi[l] = u;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    // guard of the packed scorecard: counts < 256 and sums < 2^24 per candidate
+    for (int o = 16; o; o >>= 1) isum += __shfl_xor_sync(0xffffffffu, isum, o);
+    if ((tid & 31) == 0) red[tid >> 5] = isum;
+    __syncthreads();
+    if (tid == 0) {
+        unsigned long long t = 0;
+        for (int w = 0; w < kPrepBlock / 32; w++) t += red[w];
+        a.guard[s] = ((uint64_t)n * a.maxz <= 255u && t * a.maxz < (1ull << 24)) ? 1u : 0u;
+        // sweep: windows [m-dF, m+dF] of sorted peaks start and end in the same order
+        Interval *out = a.ivl + 2ull * q0;
+        uint32_t nv = 0, c = 0, S = 0;
+        int is = 0, ie = 0;
+        int64_t prev = 0;
+        const int64_t dF = a.dF;
+        while (ie < n) {
+            const int64_t ps = is < n ? (int64_t)pk[is] - dF : INT64_MAX;
+            const int64_t pe = (int64_t)pk[ie] + dF + 1;
+            const int64_t pos = ps < pe ? ps : pe;
+            if (c > 0) out[nv++] = Interval{(uint32_t)prev, (uint32_t)(pos - 1), c, S};
+            while (ie < n && (int64_t)pk[ie] + dF + 1 == pos) { c--; S -= pi[ie]; ie++; }
+            while (is < n && (int64_t)pk[is] - dF == pos) { c++; S += pi[is]; is++; }
+            prev = pos;
+        }
+        a.nivl[s] = nv;
+        nv_s = nv;
+    }
+    __syncthreads();
+    // windows and scan volume
+    const double dM = a.dMq ? a.dMq[s] : a.dM;
+    const float pr = a.prec[s];
+    const float p1 = __double2float_rn(__dsub_rn((double)pr, dM));
+    const float p2 = __double2float_rn(__dadd_rn((double)pr, dM));
+    unsigned long long vol = 0;
+    const uint32_t nv = nv_s;
+    const Interval *iv = a.ivl + 2ull * q0;
+    for (int l = 0; l < a.nlen; l++) {
+        const DevLen ln = a.lens[l];
+        int lo = 1, hi = 0;
+        if (!(dM < 0.0) && ln.npep > 0) {
+            const float *m = a.mass + ln.mass_off;
+            const uint32_t N = ln.npep;
+            if (p1 == p1 && p2 == p2 && !(p1 > m[N - 1]) && !(p2 < m[0])) {
+                uint32_t x = 0, y = N;
+                while (x < y) { const uint32_t c = (x + y) >> 1; if (m[c] < p1) x = c + 1; else y = c; }
+                lo = (int)x;
+                x = 0; y = N;
+                while (x < y) { const uint32_t c = (x + y) >> 1; if (p2 < m[c]) y = c; else x = c + 1; }
+                hi = (int)x - 1;
+            }
+        }
+        if (tid == 0) win[(uint64_t)s * a.nlen + l] = make_int2(lo, hi);
+        if (hi >= lo) {
+            const uint32_t W = (uint32_t)(hi - lo + 1);
+            const uint32_t ntiles = (W + (uint32_t)a.tile - 1) / (uint32_t)a.tile;
+            const uint32_t *bA = a.bA + (uint64_t)l * a.nbins;
+            for (uint32_t i = tid; i < nv; i += kPrepBlock)
+                vol += (unsigned long long)(__ldg(bA + iv[i].b1 + 1) - __ldg(bA + iv[i].b0)) * ntiles;
+            if (tid == 0) vol += W;
+        }
+    }
+    for (int o = 16; o; o >>= 1) vol += __shfl_xor_sync(0xffffffffu, vol, o);
+    __syncthreads();
+    if ((tid & 31) == 0) red[tid >> 5] = vol;
+    __syncthreads();
+    if (tid == 0) {
+        unsigned long long t = 0;
+        for (int w = 0; w < kPrepBlock / 32; w++) t += red[w];
+        work_key[s] = t;
+        order0[s] = s;
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// k_search_batched
+// ------------------------------------------------------------------------------------
+constexpr int kBBlock = 1024;
+constexpr int kBWarps = kBBlock / 32;
+constexpr int kPend = 64;       // per-warp queue of candidates awaiting a hyperscore
+constexpr int kIvlChunk = 1024; // intervals per span table
+constexpr int kUnit = 1024;     // ids per warp work unit (32 per lane)
+constexpr int kIlp = 8;         // iA loads in flight per lane
+
+// Dynamic shared memory after the scorecard tile:
+//   queued candidates a = packed word (or wide counts | b-sum << 32),
+//                     b = candidate offset in the tile | wide y-sum << 32;
+//   span table of the current length: iA start, flat prefix and (S, c) per interval.
+struct BatchDyn {
+    unsigned long long (*pend_a)[kPend];
+    unsigned long long (*pend_b)[kPend];
+    uint32_t *sp_start;
+    uint32_t *sp_pre;
+    uint2 *sp_cs;
+};
+
+__host__ __device__ constexpr size_t batch_dyn_bytes() {
+    return sizeof(unsigned long long) * kBWarps * kPend * 2 + sizeof(uint2) * kIvlChunk +
+           sizeof(uint32_t) * (2 * kIvlChunk + 4);
+}
+
+__device__ __forceinline__ BatchDyn carve_dyn(unsigned char *base)
+{
+    BatchDyn d;
+    d.pend_a = reinterpret_cast<unsigned long long (*)[kPend]>(base);
+    base += sizeof(unsigned long long) * kBWarps * kPend;
+    d.pend_b = reinterpret_cast<unsigned long long (*)[kPend]>(base);
+    base += sizeof(unsigned long long) * kBWarps * kPend;
+    d.sp_cs = reinterpret_cast<uint2 *>(base);
+    base += sizeof(uint2) * kIvlChunk;
+    d.sp_start = reinterpret_cast<uint32_t *>(base);
+    base += sizeof(uint32_t) * kIvlChunk;
+    d.sp_pre = reinterpret_cast<uint32_t *>(base);
+    return d;
+}
+
+struct BatchSmem {
+    uint32_t hist[kHist];
+    double lgf[81];
+    Cell heap[kMaxHeap + 1];
+
+    uint32_t scan_tmp[kBWarps];
+    int32_t warp_cnt[kBWarps];
+    int32_t heap_size;
+    int32_t cpsms;
+    int32_t status;
+    int32_t spec;
+    uint32_t next_unit;
+    float root;
+};
+
+__device__ __forceinline__ void scatter_packed(unsigned long long *sc, uint32_t id, uint32_t idlo, uint32_t span,
+                                               uint32_t speclen, uint32_t half, uint32_t magic, uint32_t vb)
+{
+    const uint32_t rel = id - idlo;
+    if (rel < span) {
+        const uint32_t cand = div_speclen(rel, speclen, magic);
+        const uint32_t pos = rel - cand * speclen;
+        atomicAdd(sc + cand, pos >= half ? ((unsigned long long)vb << 32) : (unsigned long long)vb);
+    }
+}
+
+__device__ __forceinline__ void scatter_wide(uint32_t *cnt, uint32_t *ib, uint32_t *iy, uint32_t id, uint32_t idlo,
+                                             uint32_t span, uint32_t speclen, uint32_t half, uint32_t magic,
+                                             uint32_t c, uint32_t S)
+{
+    const uint32_t rel = id - idlo;
+    if (rel < span) {
+        const uint32_t cand = div_speclen(rel, speclen, magic);
+        const bool y = rel - cand * speclen >= half;
+        atomicAdd(cnt + cand, y ? (c << 16) : c);
+        atomicAdd((y ? iy : ib) + cand, S);
+    }
+}
+
+// Hyperscores of up to 32 queued candidates (one per lane), in queue order: the
+// histogram and candidate count take every PSM; PSMs with h >= tau go, in order, to
+// the warp's entrant list for the exact heap.
+__device__ __forceinline__ void score_queue(BatchSmem &sm, const BatchDyn &dd, const SearchArgs &a, int wid, int lane,
+                                            int n, int t0,
+                                            int ixx, uint32_t speclen, float tau, bool wide, Cell *ent, int &nent,
+                                            int &cps)
+{
+    bool psm = false;
+    Cell cell;
+    if (lane < n) {
+        const unsigned long long va = dd.pend_a[wid][lane], vb = dd.pend_b[wid][lane];
+        uint32_t bc, yc, ib, iy;
+        if (!wide) {
+            const uint32_t lo = (uint32_t)va, hi = (uint32_t)(va >> 32);
+            bc = lo >> 24; ib = lo & 0xFFFFFFu; yc = hi >> 24; iy = hi & 0xFFFFFFu;
+        } else {
+            bc = (uint32_t)va & 0xFFFFu; yc = (uint32_t)va >> 16;
+            ib = (uint32_t)(va >> 32); iy = (uint32_t)(vb >> 32);
+        }
+        uint32_t bi = bc, yi = yc;
+        if (bi > 80u || yi > 80u) {
+            atomicOr(&sm.status, 4);
+            bi = min(bi, 80u);
+            yi = min(yi, 80u);
+        }
+        const double h1 = sm.lgf[bi] + sm.lgf[yi];
+        float h = __double2float_rn(h1 + log10((double)(uint32_t)(1u + ib)) + log10((double)(uint32_t)(1u + iy)) -
+                                    4.0);
+        if (h > 0.0f) {
+            if (h >= 80.0f) h = 79.0f;
+            psm = true;
+            cell.h = h;
+            cell.psid = t0 + (int)(uint32_t)vb;
+            cell.ixx = (uint16_t)ixx;
+            cell.shp = (uint16_t)((bc + yc) & 0xFFFFu);
+            cell.total = (uint16_t)speclen;
+            cell.pad = 0;
+            const int hb = __double2int_rz(__dadd_rn((double)__fmul_rn(h, 10.0f), 0.5));
+            atomicAdd(&sm.hist[hb], 1u);
+        }
+    }
+    const unsigned pb = __ballot_sync(0xffffffffu, psm);
+    cps += __popc(pb);
+    const bool e = psm && cell.h >= tau;
+    const unsigned eb = __ballot_sync(0xffffffffu, e);
+    if (e) ent[nent + __popc(eb & ((1u << lane) - 1u))] = cell;
+    nent += __popc(eb);
+}
+
+// Span table of up to kIvlChunk intervals for one length: iA start of each interval's
+// bins, exclusive prefix of their id counts (the flat id space), coverage (S, c).
+__device__ __forceinline__ void build_span_table(BatchSmem &sm, const BatchDyn &dd, const Interval *iv, uint32_t n,
+                                                 const uint32_t *__restrict__ bA, int tid, int lane, int wid)
+{
+    uint32_t cnt = 0;
+    if (tid < (int)n) {
+        const Interval v = iv[tid];
+        const uint32_t b = __ldg(bA + v.b0), e = __ldg(bA + v.b1 + 1);
+        dd.sp_start[tid] = b;
+        dd.sp_cs[tid] = make_uint2(v.S, v.c);
+        cnt = e - b;
+    }
+    // block exclusive scan of cnt (kBBlock == kIvlChunk)
+    uint32_t x = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) sm.scan_tmp[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        uint32_t t = sm.scan_tmp[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
+        }
+        sm.scan_tmp[lane] = t;
+    }
+    __syncthreads();
+    const uint32_t incl = x + (wid ? sm.scan_tmp[wid - 1] : 0u);
+    if (tid < (int)n) dd.sp_pre[tid] = incl - cnt;
+    if (tid == (int)n - 1) dd.sp_pre[n] = incl;
+    if (n == 0 && tid == 0) dd.sp_pre[0] = 0;
+}
+
+__global__ void __launch_bounds__(kBBlock, 1) k_search_batched(SearchArgs a)
+{
+    extern __shared__ __align__(16) unsigned char dyn[];
+    __shared__ BatchSmem sm;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    for (int i = tid; i < 81; i += kBBlock) sm.lgf[i] = a.lgfact[i];
+    const int T = a.tile;
+    unsigned long long *scp = reinterpret_cast<unsigned long long *>(dyn);
+    const BatchDyn dd = carve_dyn(dyn + (size_t)T * 8);
+    for (int i = tid; i < 2 * T; i += kBBlock) reinterpret_cast<uint32_t *>(dyn)[i] = 0;
+    // this warp's entrant list (global scratch, one slot per candidate of its range)
+    Cell *ent = a.spill + ((uint64_t)blockIdx.x * kBWarps + wid) * (uint64_t)a.spill_per_warp;
+
+    for (;;) {
+        __syncthreads();
+        if (tid == 0) {
+            const uint32_t slot = atomicAdd(a.queue, 1u);
+            sm.spec = slot < a.nspec ? (int32_t)a.order[slot] : -1;
+            sm.heap_size = 0;
+            sm.cpsms = 0;
+            sm.status = 0;
+            sm.root = 0.0f;
+        }
+        for (int i = tid; i < kHist; i += kBBlock) sm.hist[i] = 0;
+        __syncthreads();
+        const int s = sm.spec;
+        if (s < 0) break;
+        if (a.nivl[s] == 0) {                 // no probed bins, or flagged by k_prep
+            if (tid == 0) {
+                gx_result r;
+                memset(&r, 0, sizeof(r));
+                a.out[s] = r;
+            }
+            for (int i = tid; i < kHist; i += kBBlock) a.hist_g[(uint64_t)s * kHist + i] = 0;
+            if (a.heap_out)
+                for (int i = tid; i < a.heap_cap; i += kBBlock) a.heap_out[(uint64_t)s * a.heap_cap + i] = gx_cell{};
+            continue;
+        }
+        const bool wide = a.guard[s] == 0 || (a.flags & GX_FLAG_WIDE_SCORECARD);
+        if (tid == 0 && wide) sm.status |= 8;
+        const int ctile = wide ? (T * 2) / 3 : T;
+        uint32_t *scw_cnt = reinterpret_cast<uint32_t *>(dyn);
+        uint32_t *scw_ib = scw_cnt + ctile;
+        uint32_t *scw_iy = scw_ib + ctile;
+        const uint32_t nv = a.nivl[s];
+        const Interval *ivl = a.ivl + 2ull * a.qidx[s];
+        int cps = 0;   // candidate PSMs counted by this warp (lane 0 adds them at the end)
+
+        for (int ixx = 0; ixx < a.nlen; ixx++) {
+            const int2 w = a.win[(uint64_t)s * a.nlen + ixx];
+            if (w.y < w.x) continue;
+            const DevLen ln = a.lens[ixx];
+            const uint32_t *__restrict__ bA = a.bA + (uint64_t)ixx * a.nbins;
+            const uint32_t *__restrict__ iA = a.iA + ln.ia_off;
+            const uint32_t speclen = ln.speclen, half = ln.half, magic = ln.magic;
+            const uint32_t W = (uint32_t)(w.y - w.x + 1);
+            const uint32_t ntiles = (W + ctile - 1) / ctile;
+            const uint32_t tsz = (W + ntiles - 1) / ntiles;   // balanced tiles
+            for (uint32_t ti = 0; ti < ntiles; ti++) {
+                const int t0 = w.x + (int)(ti * tsz);
+                const int t1 = min(w.y + 1, t0 + (int)tsz);
+                const int tn = t1 - t0;
+                if (tn <= 0) continue;
+                const uint32_t idlo = (uint32_t)t0 * speclen, span = (uint32_t)tn * speclen;
+                // ---- stream every interval's iA span into the scorecard -----------------
+                for (uint32_t ic0 = 0; ic0 < nv; ic0 += kIvlChunk) {
+                    const uint32_t ncv = min((uint32_t)kIvlChunk, nv - ic0);
+                    if (ti == 0 || nv > (uint32_t)kIvlChunk)
+                        build_span_table(sm, dd, ivl + ic0, ncv, bA, tid, lane, wid);
+                    if (tid == 0) sm.next_unit = 0;
+                    __syncthreads();
+                    const uint32_t M = dd.sp_pre[ncv];
+                    for (;;) {
+                        uint32_t u = 0;
+                        if (lane == 0) u = atomicAdd(&sm.next_unit, 1u);
+                        u = __shfl_sync(0xffffffffu, u, 0);
+                        const uint32_t f0 = u * (uint32_t)kUnit;
+                        if (f0 >= M) break;
+                        const uint32_t f1 = min(M, f0 + (uint32_t)kUnit);
+                        // interval of the unit's first id (same for all lanes)
+                        uint32_t lo = 0, hi = ncv;
+                        while (hi - lo > 1) {
+                            const uint32_t mid = (lo + hi) >> 1;
+                            if (dd.sp_pre[mid] <= f0) lo = mid; else hi = mid;
+                        }
+                        uint32_t k = lo;
+                        for (uint32_t g = f0 + lane; g < f1; g += 32 * kIlp) {
+                            uint32_t idv[kIlp], vv[kIlp];
+                            bool ok[kIlp];
+#pragma unroll
+                            for (int j = 0; j < kIlp; j++) {
+                                const uint32_t f = g + 32u * j;
+                                ok[j] = f < f1;
+                                if (ok[j]) {
+                                    while (dd.sp_pre[k + 1] <= f) k++;
+                                    idv[j] = __ldg(iA + dd.sp_start[k] + (f - dd.sp_pre[k]));
+                                    const uint2 cs = dd.sp_cs[k];
+                                    vv[j] = wide ? k : ((cs.y << 24) | cs.x);
+                                }
+                            }
+#pragma unroll
+                            for (int j = 0; j < kIlp; j++) {
+                                if (!ok[j]) continue;
+                                if (!wide) {
+                                    scatter_packed(scp, idv[j], idlo, span, speclen, half, magic, vv[j]);
+                                } else {
+                                    const uint2 cs = dd.sp_cs[vv[j]];
+                                    scatter_wide(scw_cnt, scw_ib, scw_iy, idv[j], idlo, span, speclen, half, magic,
+                                                 cs.y, cs.x);
+                                }
+                            }
+                        }
+                    }
+                    __syncthreads();
+                }
+                // ---- scan: each warp owns a contiguous range, in entry order ------------
+                const float tau = sm.heap_size < a.heap_cap ? -1.0f : sm.root;
+                const int R = (tn + kBWarps - 1) / kBWarps;
+                const int r0 = min(tn, wid * R), r1 = min(tn, r0 + R);
+                int npend = 0, nent = 0;
+                for (int base = r0; base < r1; base += 32) {
+                    const int c = base + lane;
+                    bool is = false;
+                    unsigned long long va = 0ull, vb = 0ull;
+                    if (c < r1) {
+                        uint32_t bc, yc;
+                        if (!wide) {
+                            va = scp[c];
+                            scp[c] = 0ull;
+                            bc = ((uint32_t)va) >> 24;
+                            yc = (uint32_t)(va >> 32) >> 24;
+                            vb = (uint32_t)c;
+                        } else {
+                            const uint32_t cnt = scw_cnt[c];
+                            bc = cnt & 0xFFFFu;
+                            yc = cnt >> 16;
+                            va = (unsigned long long)cnt | ((unsigned long long)scw_ib[c] << 32);
+                            vb = (unsigned long long)(uint32_t)c | ((unsigned long long)scw_iy[c] << 32);
+                            scw_cnt[c] = 0; scw_ib[c] = 0; scw_iy[c] = 0;
+                        }
+                        is = ((bc + yc) & 0xFFFFu) >= a.min_shp;
+                    }
+                    const unsigned bal = __ballot_sync(0xffffffffu, is);
+                    if (is) {
+                        const int slot = npend + __popc(bal & ((1u << lane) - 1u));
+                        dd.pend_a[wid][slot] = va;
+                        dd.pend_b[wid][slot] = vb;
+                    }
+                    npend += __popc(bal);
+                    __syncwarp();
+                    if (npend >= 32) {
+                        score_queue(sm, dd, a, wid, lane, 32, t0, ixx, speclen, tau, wide, ent, nent, cps);
+                        __syncwarp();
+                        if (lane < npend - 32) {
+                            dd.pend_a[wid][lane] = dd.pend_a[wid][32 + lane];
+                            dd.pend_b[wid][lane] = dd.pend_b[wid][32 + lane];
+                        }
+                        npend -= 32;
+                        __syncwarp();
+                    }
+                }
+                if (npend > 0) score_queue(sm, dd, a, wid, lane, npend, t0, ixx, speclen, tau, wide, ent, nent, cps);
+                if (lane == 0) sm.warp_cnt[wid] = nent;
+                __syncthreads();
+                // ---- exact heap: entrants of all warps, in entry order ------------------
+                if (tid == 0) {
+                    int hs = sm.heap_size;
+                    for (int w2 = 0; w2 < kBWarps; w2++) {
+                        const Cell *e2 = a.spill + ((uint64_t)blockIdx.x * kBWarps + w2) * (uint64_t)a.spill_per_warp;
+                        const int n2 = sm.warp_cnt[w2];
+                        for (int k = 0; k < n2; k++) heap_insert(sm.heap, hs, a.heap_cap, e2[k]);
+                    }
+                    sm.heap_size = hs;
+                    sm.root = sm.heap[0].h;
+                }
+            }
+        }
+        if (lane == 0 && cps) atomicAdd(&sm.cpsms, cps);
+        __syncthreads();
+        // ---- per-spectrum outputs (the tail fit runs in k_tailfit) -------------------
+        for (int i = tid; i < kHist; i += kBBlock) a.hist_g[(uint64_t)s * kHist + i] = sm.hist[i];
+        if (a.heap_out)
+            for (int i = tid; i < a.heap_cap; i += kBBlock) {
+                gx_cell o{};
+                if (i < sm.heap_size) {
+                    const Cell c = sm.heap[i];
+                    o.hyperscore = c.h; o.psid = c.psid; o.idxoffset = c.ixx; o.sharedions = c.shp;
+                    o.totalions = c.total;
+                }
+                a.heap_out[(uint64_t)s * a.heap_cap + i] = o;
+            }
+        if (tid == 0) {
+            gx_result r;
+            memset(&r, 0, sizeof(r));
+            r.cpsms = sm.cpsms;
+            r.status = sm.status;
+            if ((uint32_t)sm.cpsms >= a.min_cpsm) {
+                const Cell t = heap_getmax(sm.heap, sm.heap_size);
+                r.top.hyperscore = t.h; r.top.psid = t.psid; r.top.idxoffset = t.ixx;
+                r.top.sharedions = t.shp; r.top.totalions = t.total;
+                r.maxhyp = __double2int_rz(__dadd_rn((double)__fmul_rn(t.h, 10.0f), 0.5));
+            }
+            a.out[s] = r;
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// k_tailfit: one warp per spectrum (the FP64 fit itself is serial in lane 0)
+// ------------------------------------------------------------------------------------
+constexpr int kTfWarps = 4;
+
+__global__ void __launch_bounds__(kTfWarps * 32) k_tailfit(SearchArgs a)
+{
+    __shared__ uint32_t h[kTfWarps][kHist];
+    __shared__ double sx[kTfWarps][kHist + 2];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t s = blockIdx.x * kTfWarps + w;
+    if (s >= a.nspec) return;
+    gx_result r = a.out[s];
+    if ((uint32_t)r.cpsms < a.min_cpsm) return;
+    for (int i = lane; i < kHist; i += 32) h[w][i] = a.hist_g[(uint64_t)s * kHist + i];
+    __syncwarp();
+    if (lane == 0) {
+        tail_fit(h[w], r.cpsms, r.maxhyp, sx[w], r);
+        r.status |= 1;
+        if (r.e_x < a.expect_max) r.status |= 2;
+        a.out[s] = r;
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// host side
+// ------------------------------------------------------------------------------------
+size_t batched_sort_temp_bytes(uint32_t max_spec)
+{
+    size_t bytes = 0;
+    cub::DeviceRadixSort::SortPairsDescending(nullptr, bytes, (const uint64_t *)nullptr, (uint64_t *)nullptr,
+                                              (const uint32_t *)nullptr, (uint32_t *)nullptr, (int)max_spec);
+    return bytes;
+}
+
+size_t batched_dyn_smem(int tile) { return (size_t)tile * 8 + batch_dyn_bytes(); }
+
+cudaError_t batched_set_attributes(int tile)
+{
+    return cudaFuncSetAttribute(k_search_batched, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)batched_dyn_smem(tile));
+}
+
+cudaError_t launch_batched(SearchArgs a, const BatchedScratch &b, cudaStream_t st)
+{
+    cudaError_t e;
+    int h = prof_begin("k_prep", st);
+    k_prep<<<a.nspec, kPrepBlock, 0, st>>>(a, const_cast<int2 *>(a.win), b.key_in, b.ord_in);
+    prof_end(h, st);
+    count_launch();
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    size_t tb = b.sort_temp_bytes;
+    h = prof_begin("sort_by_volume", st);
+    e = cub::DeviceRadixSort::SortPairsDescending(b.sort_temp, tb, b.key_in, b.key_out, b.ord_in, b.ord_out,
+                                                  (int)a.nspec, 0, 64, st);
+    prof_end(h, st);
+    count_launch();
+    if (e != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(a.queue, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
+    a.order = b.ord_out;
+    h = prof_begin("k_search_batched", st);
+    k_search_batched<<<b.grid, kBBlock, batched_dyn_smem(a.tile), st>>>(a);
+    prof_end(h, st);
+    count_launch();
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    h = prof_begin("k_tailfit", st);
+    k_tailfit<<<(a.nspec + kTfWarps - 1) / kTfWarps, kTfWarps * 32, 0, st>>>(a);
+    prof_end(h, st);
+    count_launch();
+    return cudaGetLastError();
+}
+
+}  // namespace gx

@@ -1,0 +1,25 @@
+// Host-side entry points of the batched query path (gx_batched.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "gx_device.cuh"
+
+namespace gx {
+
+// Scratch the batched path needs beyond SearchArgs.
+struct BatchedScratch {
+    uint64_t *key_in, *key_out;   // scan volume per spectrum (sort keys)
+    uint32_t *ord_in, *ord_out;   // spectrum ids
+    void *sort_temp;
+    size_t sort_temp_bytes;
+    int grid;                     // persistent CTAs
+};
+
+size_t batched_sort_temp_bytes(uint32_t max_spec);
+cudaError_t batched_set_attributes(int tile);
+cudaError_t launch_batched(SearchArgs a, const BatchedScratch &b, cudaStream_t st);
+
+}  // namespace gx

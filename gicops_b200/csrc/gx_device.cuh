@@ -18,6 +18,34 @@ struct DevLen {
     uint32_t speclen;     // ions per entry
     uint32_t half;        // speclen / 2 (b ions first, then y ions)
     uint32_t peplen;
+    uint32_t magic;       // ceil(2^32 / speclen): id / speclen = umulhi(id, magic), minus one if over
+    uint32_t pad;
+};
+
+// Exact id / speclen for any 32-bit id: umulhi with ceil(2^32/d) is at most one too large.
+__device__ __forceinline__ uint32_t div_speclen(uint32_t id, uint32_t d, uint32_t magic)
+{
+    uint32_t q = __umulhi(id, magic);
+    if ((uint64_t)q * d > id) q--;
+    return q;
+}
+
+// A run of consecutive fragment bins [b0, b1] covered by the same set of peak
+// windows: c peaks, intensity sum S (mod 2^32).
+struct Interval {
+    uint32_t b0, b1;
+    uint32_t c;
+    uint32_t S;
+};
+
+// One heap cell as kept on chip.
+struct Cell {
+    float h;
+    int32_t psid;
+    uint16_t ixx;
+    uint16_t shp;
+    uint16_t total;
+    uint16_t pad;
 };
 
 // Everything a search launch reads.
@@ -49,20 +77,21 @@ struct SearchArgs {
     const double *lgfact; // [81]
     // scratch / outputs
     const int2 *win;      // [nspec * nlen] candidate window per (spectrum, length)
+    // batched path
+    Interval *ivl;        // [2 * npeaks]: intervals of spectrum s start at 2 * qidx[s]
+    uint64_t ivl_cap;     // intervals the buffer holds
+    uint32_t *nivl;       // [nspec]
+    uint32_t *guard;      // [nspec]: 1 if the packed scorecard is exact for the spectrum
+    const uint32_t *order;// [nspec] spectra, heaviest first
+    uint32_t *queue;      // work-queue head
+    uint32_t *hist_g;     // [nspec * kHist] histograms (always)
+    int32_t tile;         // candidates per scorecard tile
+    Cell *spill;          // [grid * 32 warps * spill_per_warp] heap entrants of each warp's range
+    uint32_t spill_per_warp;
     gx_result *out;
     gx_cell *heap_out;    // optional [nspec * heap_cap]
     uint32_t *hist_out;   // optional [nspec * kHist]
     int32_t *err;         // device guard word
-};
-
-// One heap cell as kept on chip.
-struct Cell {
-    float h;
-    int32_t psid;
-    uint16_t ixx;
-    uint16_t shp;
-    uint16_t total;
-    uint16_t pad;
 };
 
 // ---- minHeap<hCell> of the reference (source/core/include/minheap.h:103-271) ------
@@ -113,7 +142,7 @@ __device__ __forceinline__ int32_t to_int_x86(double v)
 // expeRT::ModelTailFit (source/core/expeRT.cpp:396-559) followed by the e-value of
 // source/core/dslim_query.cpp:1017-1061.  Serial FP64 in one thread; the sums run in
 // the reference's order so the fit matches it.  `sx` is scratch for kHist+1 doubles.
-__device__ void tail_fit(const uint32_t *hist, int32_t cpsms, int32_t hyp, double *sx_buf, gx_result &r)
+__device__ inline void tail_fit(const uint32_t *hist, int32_t cpsms, int32_t hyp, double *sx_buf, gx_result &r)
 {
     double mu_t = 0.0, beta_t = 4.0;
     int end1 = hyp - 1;

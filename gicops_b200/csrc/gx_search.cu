@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/gicops_b200.h"
+#include "gx_batched.h"
 #include "gx_device.cuh"
 #include "gx_internal.h"
 
@@ -377,7 +378,8 @@ struct gx_index {
 };
 
 namespace {
-constexpr int kDefaultTile = 8192;  // candidates per scorecard tile (8 B each)
+constexpr int kDefaultTile = 8192;   // plain path: candidates per scorecard tile (8 B each)
+constexpr int kBatchedTile = 22016;  // batched path: 172 KB scorecard, one CTA per SM
 }
 
 struct gx_workspace {
@@ -395,6 +397,13 @@ struct gx_workspace {
     gx_cell *heap = nullptr;
     uint32_t *hist = nullptr;
     cudaStream_t stream = nullptr;
+    // batched path
+    Interval *ivl = nullptr;
+    uint32_t *nivl = nullptr, *guard = nullptr, *queue = nullptr, *hist_g = nullptr;
+    Cell *spill = nullptr;
+    uint32_t spill_per_warp = 0;
+    BatchedScratch bs{};
+    int tile = kBatchedTile;
 };
 
 extern "C" const char *gx_last_error(void) { return g_last_error.c_str(); }
@@ -470,7 +479,8 @@ extern "C" gx_status gx_index_upload(const gx_length_desc *lens, int32_t nlen, u
         if (d.npep && (!d.mass || !d.bA || !d.iA)) return fail(GX_ERR_INVLD_PTR, "gx_index_upload: null array");
         if (d.bA && d.bA[nbins - 1] != (uint64_t)d.npep * d.speclen)
             return fail(GX_ERR_INVLD_INDEX, "gx_index_upload: bA[nbins-1] must equal npep*speclen");
-        hl[i] = DevLen{tot_ia, tot_m, d.npep, d.speclen, d.speclen / 2, d.peplen};
+        const uint32_t magic = (uint32_t)(((1ull << 32) + d.speclen - 1) / d.speclen);
+        hl[i] = DevLen{tot_ia, tot_m, d.npep, d.speclen, d.speclen / 2, d.peplen, magic, 0};
         tot_ia += (uint64_t)d.npep * d.speclen;
         tot_m += d.npep;
     }
@@ -532,8 +542,9 @@ extern "C" gx_status gx_workspace_free(gx_workspace *ws)
 {
     if (!ws) return GX_SUCCESS;
     if (ws->ix) cudaSetDevice(ws->ix->device);
-    void *ptrs[] = {ws->win, ws->lgfact, ws->err, ws->qidx, ws->moz, ws->intn, ws->charge,
-                    ws->prec, ws->dMq, ws->out, ws->heap, ws->hist};
+    void *ptrs[] = {ws->win, ws->lgfact, ws->err, ws->qidx, ws->moz, ws->intn, ws->charge, ws->prec,
+                    ws->dMq, ws->out, ws->heap, ws->hist, ws->ivl, ws->nivl, ws->guard, ws->queue,
+                    ws->hist_g, ws->spill, ws->bs.key_in, ws->bs.key_out, ws->bs.ord_in, ws->bs.ord_out, ws->bs.sort_temp};
     for (void *p : ptrs) cudaFree(p);
     if (ws->stream) cudaStreamDestroy(ws->stream);
     delete ws;
@@ -566,6 +577,26 @@ extern "C" gx_status gx_workspace_create(const gx_index *ix, uint32_t max_spec, 
     al((void **)&ws->prec, sizeof(float) * max_spec);
     al((void **)&ws->dMq, sizeof(double) * max_spec);
     al((void **)&ws->out, sizeof(gx_result) * max_spec);
+    al((void **)&ws->ivl, sizeof(Interval) * 2 * (uint64_t)(max_peaks ? max_peaks : 1));
+    al((void **)&ws->nivl, sizeof(uint32_t) * max_spec);
+    al((void **)&ws->guard, sizeof(uint32_t) * max_spec);
+    al((void **)&ws->queue, sizeof(uint32_t));
+    al((void **)&ws->hist_g, sizeof(uint32_t) * GX_HIST_BINS * (uint64_t)max_spec);
+    al((void **)&ws->bs.key_in, sizeof(uint64_t) * max_spec);
+    al((void **)&ws->bs.key_out, sizeof(uint64_t) * max_spec);
+    al((void **)&ws->bs.ord_in, sizeof(uint32_t) * max_spec);
+    al((void **)&ws->bs.ord_out, sizeof(uint32_t) * max_spec);
+    ws->bs.sort_temp_bytes = batched_sort_temp_bytes(max_spec);
+    al(&ws->bs.sort_temp, ws->bs.sort_temp_bytes);
+    if (e == cudaSuccess) {
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        ws->bs.grid = sms;
+    }
+    ws->spill_per_warp = (uint32_t)((ws->tile + 31) / 32);
+    al((void **)&ws->spill, sizeof(Cell) * (uint64_t)ws->bs.grid * 32 * ws->spill_per_warp);
+    if (e == cudaSuccess) e = batched_set_attributes(ws->tile);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -626,6 +657,17 @@ gx_status launch_search(gx_index *ix, gx_workspace *ws, const gx_queries *q, con
     a.expect_max = p->expect_max; a.flags = p->flags; a.lgfact = ws->lgfact;
     a.win = ws->win; a.out = out; a.heap_out = heap; a.hist_out = hist; a.err = ws->err;
 
+    if (!(p->flags & GX_FLAG_PLAIN)) {
+        if (q->npeaks > ws->max_peaks) return fail(GX_ERR_INVLD_SIZE, "more peaks than the workspace holds");
+        a.ivl = ws->ivl; a.ivl_cap = 2ull * ws->max_peaks; a.nivl = ws->nivl; a.guard = ws->guard; a.queue = ws->queue;
+        a.hist_g = hist ? hist : ws->hist_g;
+        a.tile = ws->tile;
+        a.spill = ws->spill;
+        a.spill_per_warp = ws->spill_per_warp;
+        cudaError_t e = launch_batched(a, ws->bs, st);
+        if (e != cudaSuccess) return cuda_fail(e, "batched search launch");
+        return GX_SUCCESS;
+    }
     const uint64_t nw = (uint64_t)q->nspec * ix->nlen;
     int h = prof_begin("k_windows", st);
     k_windows<<<(unsigned)((nw + 255) / 256), 256, 0, st>>>(a, ws->win);
