@@ -415,32 +415,30 @@ __global__ void __launch_bounds__(kBBlock, 1) k_search_batched(SearchArgs a)
                             const uint32_t mid = (lo + hi) >> 1;
                             if (dd.sp_pre[mid] <= f0) lo = mid; else hi = mid;
                         }
-                        uint32_t k = lo;
-                        for (uint32_t g = f0 + lane; g < f1; g += 32 * kIlp) {
-                            uint32_t idv[kIlp], vv[kIlp];
-                            bool ok[kIlp];
+                        // walk the unit interval by interval: bookkeeping once per interval
+                        uint32_t k = lo, f = f0;
+                        while (f < f1) {
+                            const uint32_t fe = min(f1, dd.sp_pre[k + 1]);
+                            const uint32_t delta = dd.sp_start[k] - dd.sp_pre[k];   // iA index = flat + delta (mod 2^32)
+                            const uint2 cs = dd.sp_cs[k];
+                            if (!wide) {
+                                const uint32_t vb = (cs.y << 24) | cs.x;
+                                for (uint32_t g = f + lane; g < fe; g += 32 * kIlp) {
+                                    uint32_t idv[kIlp];
 #pragma unroll
-                            for (int j = 0; j < kIlp; j++) {
-                                const uint32_t f = g + 32u * j;
-                                ok[j] = f < f1;
-                                if (ok[j]) {
-                                    while (dd.sp_pre[k + 1] <= f) k++;
-                                    idv[j] = __ldg(iA + dd.sp_start[k] + (f - dd.sp_pre[k]));
-                                    const uint2 cs = dd.sp_cs[k];
-                                    vv[j] = wide ? k : ((cs.y << 24) | cs.x);
-                                }
-                            }
+                                    for (int j = 0; j < kIlp; j++)
+                                        idv[j] = (g + 32u * j < fe) ? __ldg(iA + (g + 32u * j + delta)) : idlo - 1u;
 #pragma unroll
-                            for (int j = 0; j < kIlp; j++) {
-                                if (!ok[j]) continue;
-                                if (!wide) {
-                                    scatter_packed(scp, idv[j], idlo, span, speclen, half, magic, vv[j]);
-                                } else {
-                                    const uint2 cs = dd.sp_cs[vv[j]];
-                                    scatter_wide(scw_cnt, scw_ib, scw_iy, idv[j], idlo, span, speclen, half, magic,
-                                                 cs.y, cs.x);
+                                    for (int j = 0; j < kIlp; j++)
+                                        scatter_packed(scp, idv[j], idlo, span, speclen, half, magic, vb);
                                 }
+                            } else {
+                                for (uint32_t g = f + lane; g < fe; g += 32)
+                                    scatter_wide(scw_cnt, scw_ib, scw_iy, __ldg(iA + (g + delta)), idlo, span, speclen, half,
+                                                 magic, cs.y, cs.x);
                             }
+                            f = fe;
+                            k++;
                         }
                     }
                     __syncthreads();
