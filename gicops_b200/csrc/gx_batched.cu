@@ -218,25 +218,22 @@ struct BatchSmem {
     float root;
 };
 
-__device__ __forceinline__ void scatter_packed(unsigned long long *sc, uint32_t id, uint32_t idlo, uint32_t span,
-                                               uint32_t speclen, uint32_t half, uint32_t magic, uint32_t vb)
+// Device ids are 2*entry + (y ion); ids of the tile satisfy id - base < lim with
+// base = 2*t0, lim = 2*tn.  The scorecard keeps b ions in [0, T) and y ions in [T, 2T).
+__device__ __forceinline__ void scatter_packed(uint32_t *sc, uint32_t id, uint32_t base, uint32_t lim, uint32_t T,
+                                               uint32_t vb)
 {
-    const uint32_t rel = id - idlo;
-    if (rel < span) {
-        const uint32_t cand = div_speclen(rel, speclen, magic);
-        const uint32_t pos = rel - cand * speclen;
-        atomicAdd(sc + cand, pos >= half ? ((unsigned long long)vb << 32) : (unsigned long long)vb);
-    }
+    const uint32_t rel = id - base;
+    if (rel < lim) atomicAdd(sc + (rel >> 1) + (rel & 1u) * T, vb);
 }
 
-__device__ __forceinline__ void scatter_wide(uint32_t *cnt, uint32_t *ib, uint32_t *iy, uint32_t id, uint32_t idlo,
-                                             uint32_t span, uint32_t speclen, uint32_t half, uint32_t magic,
-                                             uint32_t c, uint32_t S)
+__device__ __forceinline__ void scatter_wide(uint32_t *cnt, uint32_t *ib, uint32_t *iy, uint32_t id, uint32_t base,
+                                             uint32_t lim, uint32_t c, uint32_t S)
 {
-    const uint32_t rel = id - idlo;
-    if (rel < span) {
-        const uint32_t cand = div_speclen(rel, speclen, magic);
-        const bool y = rel - cand * speclen >= half;
+    const uint32_t rel = id - base;
+    if (rel < lim) {
+        const uint32_t cand = rel >> 1;
+        const bool y = rel & 1u;
         atomicAdd(cnt + cand, y ? (c << 16) : c);
         atomicAdd((y ? iy : ib) + cand, S);
     }
@@ -337,7 +334,7 @@ __global__ void __launch_bounds__(kBBlock, 1) k_search_batched(SearchArgs a)
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     for (int i = tid; i < 81; i += kBBlock) sm.lgf[i] = a.lgfact[i];
     const int T = a.tile;
-    unsigned long long *scp = reinterpret_cast<unsigned long long *>(dyn);
+    uint32_t *scp = reinterpret_cast<uint32_t *>(dyn);   // packed: b words [0, T), y words [T, 2T)
     const BatchDyn dd = carve_dyn(dyn + (size_t)T * 8);
     for (int i = tid; i < 2 * T; i += kBBlock) reinterpret_cast<uint32_t *>(dyn)[i] = 0;
     // this warp's entrant list (global scratch, one slot per candidate of its range)
@@ -384,7 +381,7 @@ __global__ void __launch_bounds__(kBBlock, 1) k_search_batched(SearchArgs a)
             const DevLen ln = a.lens[ixx];
             const uint32_t *__restrict__ bA = a.bA + (uint64_t)ixx * a.nbins;
             const uint32_t *__restrict__ iA = a.iA + ln.ia_off;
-            const uint32_t speclen = ln.speclen, half = ln.half, magic = ln.magic;
+            const uint32_t speclen = ln.speclen;
             const uint32_t W = (uint32_t)(w.y - w.x + 1);
             const uint32_t ntiles = (W + ctile - 1) / ctile;
             const uint32_t tsz = (W + ntiles - 1) / ntiles;   // balanced tiles
@@ -393,7 +390,7 @@ __global__ void __launch_bounds__(kBBlock, 1) k_search_batched(SearchArgs a)
                 const int t1 = min(w.y + 1, t0 + (int)tsz);
                 const int tn = t1 - t0;
                 if (tn <= 0) continue;
-                const uint32_t idlo = (uint32_t)t0 * speclen, span = (uint32_t)tn * speclen;
+                const uint32_t idlo = 2u * (uint32_t)t0, span = 2u * (uint32_t)tn;
                 // ---- stream every interval's iA span into the scorecard -----------------
                 for (uint32_t ic0 = 0; ic0 < nv; ic0 += kIvlChunk) {
                     const uint32_t ncv = min((uint32_t)kIvlChunk, nv - ic0);
@@ -430,12 +427,12 @@ __global__ void __launch_bounds__(kBBlock, 1) k_search_batched(SearchArgs a)
                                         idv[j] = (g + 32u * j < fe) ? __ldg(iA + (g + 32u * j + delta)) : idlo - 1u;
 #pragma unroll
                                     for (int j = 0; j < kIlp; j++)
-                                        scatter_packed(scp, idv[j], idlo, span, speclen, half, magic, vb);
+                                        scatter_packed(scp, idv[j], idlo, span, (uint32_t)T, vb);
                                 }
                             } else {
                                 for (uint32_t g = f + lane; g < fe; g += 32)
-                                    scatter_wide(scw_cnt, scw_ib, scw_iy, __ldg(iA + (g + delta)), idlo, span, speclen, half,
-                                                 magic, cs.y, cs.x);
+                                    scatter_wide(scw_cnt, scw_ib, scw_iy, __ldg(iA + (g + delta)), idlo, span, cs.y,
+                                                 cs.x);
                             }
                             f = fe;
                             k++;
@@ -455,10 +452,12 @@ __global__ void __launch_bounds__(kBBlock, 1) k_search_batched(SearchArgs a)
                     if (c < r1) {
                         uint32_t bc, yc;
                         if (!wide) {
-                            va = scp[c];
-                            scp[c] = 0ull;
-                            bc = ((uint32_t)va) >> 24;
-                            yc = (uint32_t)(va >> 32) >> 24;
+                            const uint32_t wb = scp[c], wy = scp[T + c];
+                            scp[c] = 0u;
+                            scp[T + c] = 0u;
+                            va = (unsigned long long)wb | ((unsigned long long)wy << 32);
+                            bc = wb >> 24;
+                            yc = wy >> 24;
                             vb = (uint32_t)c;
                         } else {
                             const uint32_t cnt = scw_cnt[c];

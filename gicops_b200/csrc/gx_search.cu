@@ -121,6 +121,17 @@ __global__ void k_windows(SearchArgs a, int2 *win)
     win[i] = make_int2(lo, hi);
 }
 
+// Device form of the ion ids: id = entry*speclen + pos becomes 2*entry + (pos >= speclen/2),
+// i.e. entry and ion series (b = 0, y = 1).  Order inside a bucket is unchanged.
+__global__ void k_encode_ids(uint32_t *iA, uint64_t n, uint32_t speclen, uint32_t half, uint32_t magic)
+{
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t id = iA[i];
+        const uint32_t e = div_speclen(id, speclen, magic);
+        iA[i] = 2u * e + ((id - e * speclen) >= half ? 1u : 0u);
+    }
+}
+
 __device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t *__restrict__ v, uint32_t a, uint32_t b,
                                                     uint32_t key)
 {
@@ -230,11 +241,12 @@ __global__ void __launch_bounds__(kBlock) k_search_plain(SearchArgs a, int tile)
         const DevLen ln = a.lens[ixx];
         const uint32_t *__restrict__ bA = a.bA + (uint64_t)ixx * a.nbins;
         const uint32_t *__restrict__ iA = a.iA + ln.ia_off;
-        const uint32_t speclen = ln.speclen, half = ln.half;
+        const uint32_t speclen = ln.speclen;
         for (int t0 = w.x; t0 <= w.y; t0 += ctile) {
             const int t1 = min(w.y + 1, t0 + ctile);
             const int tn = t1 - t0;
-            const uint32_t idlo = (uint32_t)t0 * speclen, idhi = (uint32_t)t1 * speclen;
+            // device ids are 2*entry + (y ion): the tile is [2*t0, 2*t1)
+            const uint32_t idlo = 2u * (uint32_t)t0, idhi = 2u * (uint32_t)t1;
             // ---- probe buckets, scatter into the scorecard ----------------------------
             for (int it = tid; it < npk * W; it += kBlock) {
                 const int k = it / W;
@@ -246,9 +258,8 @@ __global__ void __launch_bounds__(kBlock) k_search_plain(SearchArgs a, int tile)
                 const uint32_t in = sm.qin[k];
                 for (uint32_t ion = x; ion < y; ion++) {
                     const uint32_t raw = __ldg(iA + ion);
-                    const uint32_t pp = raw / speclen;
-                    const uint32_t isY = (raw - pp * speclen) >= half ? 1u : 0u;
-                    const uint32_t c = pp - (uint32_t)t0;
+                    const uint32_t isY = raw & 1u;
+                    const uint32_t c = (raw >> 1) - (uint32_t)t0;
                     if (!wide) {
                         card_add_packed(scp, c, isY, in);
                     } else {
@@ -516,10 +527,17 @@ extern "C" gx_status gx_index_upload(const gx_length_desc *lens, int32_t nlen, u
             if ((e = cudaMemcpy(ix->mass + hl[i].mass_off, d.mass, sizeof(float) * d.npep, cudaMemcpyHostToDevice)) !=
                 cudaSuccess)
                 return cleanup(cuda_fail(e, "gx_index_upload mass"));
+            const uint64_t nid = (uint64_t)d.npep * d.speclen;
+            k_encode_ids<<<(unsigned)std::min<uint64_t>((nid + 255) / 256, 65535), 256>>>(ix->iA + hl[i].ia_off, nid,
+                                                                                        d.speclen, d.speclen / 2,
+                                                                                        hl[i].magic);
+            count_launch();
+            if ((e = cudaGetLastError()) != cudaSuccess) return cleanup(cuda_fail(e, "gx_index_upload encode"));
         }
     }
     if ((e = cudaMemcpy(ix->lens, hl.data(), sizeof(DevLen) * nlen, cudaMemcpyHostToDevice)) != cudaSuccess)
         return cleanup(cuda_fail(e, "gx_index_upload lens"));
+    if ((e = cudaDeviceSynchronize()) != cudaSuccess) return cleanup(cuda_fail(e, "gx_index_upload"));
     *out = ix;
     return GX_SUCCESS;
 }
