@@ -379,15 +379,18 @@ __global__ void __launch_bounds__(kBBlock, 1) k_search_batched(SearchArgs a)
             const int2 w = a.win[(uint64_t)s * a.nlen + ixx];
             if (w.y < w.x) continue;
             const DevLen ln = a.lens[ixx];
-            const uint32_t *__restrict__ bA = a.bA + (uint64_t)ixx * a.nbins;
-            const uint32_t *__restrict__ iA = a.iA + ln.ia_off;
+            const uint32_t *__restrict__ iA = a.iAb + ln.ia_off;   // block layout
             const uint32_t speclen = ln.speclen;
-            const uint32_t W = (uint32_t)(w.y - w.x + 1);
-            const uint32_t ntiles = (W + ctile - 1) / ctile;
-            const uint32_t tsz = (W + ntiles - 1) / ntiles;   // balanced tiles
-            for (uint32_t ti = 0; ti < ntiles; ti++) {
-                const int t0 = w.x + (int)(ti * tsz);
-                const int t1 = min(w.y + 1, t0 + (int)tsz);
+            const int64_t E = a.block;
+            const int64_t kb0 = w.x / E, kb1 = w.y / E;
+            for (int64_t kb = kb0; kb <= kb1; kb++) {
+              // one block of entries = one candidate tile (two sub-tiles for the wide scorecard)
+              const uint32_t *__restrict__ bA = a.blkA + ln.blk_off + (uint64_t)kb * (a.nbins + 1);
+              const int bt0 = (int)max((int64_t)w.x, kb * E), bt1 = (int)min((int64_t)w.y + 1, (kb + 1) * E);
+              const int nsub = (bt1 - bt0 + ctile - 1) / ctile;
+              for (int ti = 0; ti < nsub; ti++) {
+                const int t0 = bt0 + ti * ctile;
+                const int t1 = min(bt1, t0 + ctile);
                 const int tn = t1 - t0;
                 if (tn <= 0) continue;
                 const uint32_t idlo = 2u * (uint32_t)t0, span = 2u * (uint32_t)tn;
@@ -502,6 +505,7 @@ __global__ void __launch_bounds__(kBBlock, 1) k_search_batched(SearchArgs a)
                     sm.heap_size = hs;
                     sm.root = sm.heap[0].h;
                 }
+              }
             }
         }
         if (lane == 0 && cps) atomicAdd(&sm.cpsms, cps);

@@ -19,7 +19,8 @@ struct DevLen {
     uint32_t half;        // speclen / 2 (b ions first, then y ions)
     uint32_t peplen;
     uint32_t magic;       // ceil(2^32 / speclen): id / speclen = umulhi(id, magic), minus one if over
-    uint32_t pad;
+    uint32_t nblk;        // entry blocks of the block layout
+    uint64_t blk_off;     // first offset table of this length in blkA
 };
 
 // Exact id / speclen for any 32-bit id: umulhi with ceil(2^32/d) is at most one too large.
@@ -52,7 +53,10 @@ struct Cell {
 struct SearchArgs {
     // index
     const uint32_t *bA;   // [nlen * nbins]
-    const uint32_t *iA;
+    const uint32_t *iA;   // bin-major CSR ids (device form 2*entry + y)
+    const uint32_t *iAb;  // block layout: per block of `block` entries, a CSR over bins
+    const uint32_t *blkA; // block layout offsets [nblk][nbins + 1] per length (relative to ia_off)
+    uint32_t block;       // entries per block
     const float *mass;
     const DevLen *lens;
     int32_t nlen;

@@ -1,0 +1,28 @@
+// Device-resident index (opaque gx_index of the C ABI).
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "gx_device.cuh"
+
+namespace gx {
+// Entries per block of the block layout; the batched path's scorecard holds one block.
+constexpr int kBlockEntries = 22016;
+}  // namespace gx
+
+struct gx_index {
+    int device = 0;
+    int32_t nlen = 0;
+    uint32_t nbins = 0;
+    uint32_t maxz = 0;
+    uint32_t block = gx::kBlockEntries;
+    uint32_t *bA = nullptr;    // [nlen][nbins] bin-major CSR offsets (the reference's bA)
+    uint32_t *iA = nullptr;    // bin-major ion ids, device form 2*entry + (y ion)
+    uint32_t *iAb = nullptr;   // the same ids in block layout
+    uint32_t *blkA = nullptr;  // block layout offsets
+    float *mass = nullptr;
+    gx::DevLen *lens = nullptr;
+    std::vector<gx::DevLen> hlens;
+    uint64_t bytes = 0;
+};

@@ -12,6 +12,9 @@ namespace gx {
 // Records `msg` as the calling thread's last error and returns `code`.
 gx_status fail(gx_status code, const std::string &msg);
 
+// Records a CUDA failure (message "what: cuda error string") and returns GX_ERR_CUDA.
+gx_status cuda_fail(int cuda_error, const char *what);
+
 // Number of kernels launched so far by this library.
 void count_launch(uint64_t n = 1);
 

@@ -19,6 +19,7 @@
 
 #include "../../include/gicops_b200.h"
 #include "gx_batched.h"
+#include "gx_index.cuh"
 #include "gx_device.cuh"
 #include "gx_internal.h"
 
@@ -69,9 +70,9 @@ void prof_end(int h, void *stream)
     if (h < (int)g_prof.size()) cudaEventRecord(g_prof[h].b, st);
 }
 
-static gx_status cuda_fail(cudaError_t e, const char *what)
+gx_status cuda_fail(int e, const char *what)
 {
-    return fail(GX_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    return fail(GX_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString((cudaError_t)e));
 }
 
 #define GX_CUDA(call)                                       \
@@ -119,17 +120,6 @@ __global__ void k_windows(SearchArgs a, int2 *win)
         }
     }
     win[i] = make_int2(lo, hi);
-}
-
-// Device form of the ion ids: id = entry*speclen + pos becomes 2*entry + (pos >= speclen/2),
-// i.e. entry and ion series (b = 0, y = 1).  Order inside a bucket is unchanged.
-__global__ void k_encode_ids(uint32_t *iA, uint64_t n, uint32_t speclen, uint32_t half, uint32_t magic)
-{
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t id = iA[i];
-        const uint32_t e = div_speclen(id, speclen, magic);
-        iA[i] = 2u * e + ((id - e * speclen) >= half ? 1u : 0u);
-    }
 }
 
 __device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t *__restrict__ v, uint32_t a, uint32_t b,
@@ -375,22 +365,8 @@ __global__ void __launch_bounds__(kBlock) k_search_plain(SearchArgs a, int tile)
 // ------------------------------------------------------------------------------------
 using namespace gx;
 
-struct gx_index {
-    int device = 0;
-    int32_t nlen = 0;
-    uint32_t nbins = 0;
-    uint32_t maxz = 0;
-    uint32_t *bA = nullptr;
-    uint32_t *iA = nullptr;
-    float *mass = nullptr;
-    DevLen *lens = nullptr;
-    std::vector<DevLen> hlens;
-    uint64_t bytes = 0;
-};
-
 namespace {
 constexpr int kDefaultTile = 8192;   // plain path: candidates per scorecard tile (8 B each)
-constexpr int kBatchedTile = 22016;  // batched path: 172 KB scorecard, one CTA per SM
 }
 
 struct gx_workspace {
@@ -414,7 +390,7 @@ struct gx_workspace {
     Cell *spill = nullptr;
     uint32_t spill_per_warp = 0;
     BatchedScratch bs{};
-    int tile = kBatchedTile;
+    int tile = kBlockEntries;
 };
 
 extern "C" const char *gx_last_error(void) { return g_last_error.c_str(); }
@@ -468,93 +444,7 @@ extern "C" int32_t gx_heap_capacity(uint32_t topmatches)
     return (int32_t)((1u << num) - 1u);
 }
 
-extern "C" gx_status gx_index_upload(const gx_length_desc *lens, int32_t nlen, uint32_t nbins, int32_t device,
-                                     gx_index **out)
-{
-    if (!lens || !out) return fail(GX_ERR_INVLD_PTR, "gx_index_upload: null argument");
-    *out = nullptr;
-    if (nlen < 1 || nlen > GX_MAX_LENGTHS || nbins < 2)
-        return fail(GX_ERR_INVLD_PARAM, "gx_index_upload: nlen must be 1..64 and nbins >= 2");
-    uint32_t maxz = 0;
-    uint64_t tot_ia = 0, tot_m = 0;
-    std::vector<DevLen> hl(nlen);
-    for (int i = 0; i < nlen; i++) {
-        const gx_length_desc &d = lens[i];
-        if (d.peplen < 2 || d.speclen < 2 || d.speclen % (2 * (d.peplen - 1)) != 0)
-            return fail(GX_ERR_INVLD_INDEX, "gx_index_upload: speclen must be 2*(L-1)*maxz");
-        const uint32_t z = d.speclen / (2 * (d.peplen - 1));
-        if (maxz && z != maxz) return fail(GX_ERR_INVLD_INDEX, "gx_index_upload: lengths disagree on maxz");
-        maxz = z;
-        if ((uint64_t)d.npep * d.speclen >= (1ull << 32))
-            return fail(GX_ERR_INVLD_SIZE, "gx_index_upload: more than 2^32 ion ids in one length");
-        if (d.npep && (!d.mass || !d.bA || !d.iA)) return fail(GX_ERR_INVLD_PTR, "gx_index_upload: null array");
-        if (d.bA && d.bA[nbins - 1] != (uint64_t)d.npep * d.speclen)
-            return fail(GX_ERR_INVLD_INDEX, "gx_index_upload: bA[nbins-1] must equal npep*speclen");
-        const uint32_t magic = (uint32_t)(((1ull << 32) + d.speclen - 1) / d.speclen);
-        hl[i] = DevLen{tot_ia, tot_m, d.npep, d.speclen, d.speclen / 2, d.peplen, magic, 0};
-        tot_ia += (uint64_t)d.npep * d.speclen;
-        tot_m += d.npep;
-    }
-    GX_CUDA(cudaSetDevice(device));
-    auto *ix = new gx_index();
-    ix->device = device;
-    ix->nlen = nlen;
-    ix->nbins = nbins;
-    ix->maxz = maxz;
-    ix->hlens = hl;
-    auto cleanup = [&](gx_status st) {
-        gx_index_free(ix);
-        return st;
-    };
-    cudaError_t e;
-    if ((e = cudaMalloc(&ix->bA, sizeof(uint32_t) * (uint64_t)nbins * nlen)) != cudaSuccess ||
-        (e = cudaMalloc(&ix->iA, sizeof(uint32_t) * (tot_ia ? tot_ia : 1))) != cudaSuccess ||
-        (e = cudaMalloc(&ix->mass, sizeof(float) * (tot_m ? tot_m : 1))) != cudaSuccess ||
-        (e = cudaMalloc(&ix->lens, sizeof(DevLen) * nlen)) != cudaSuccess) {
-        cudaGetLastError();
-        return cleanup(fail(GX_ERR_BAD_MEM_ALLOC, std::string("gx_index_upload: ") + cudaGetErrorString(e)));
-    }
-    ix->bytes = sizeof(uint32_t) * ((uint64_t)nbins * nlen + tot_ia) + sizeof(float) * tot_m + sizeof(DevLen) * nlen;
-    for (int i = 0; i < nlen; i++) {
-        const gx_length_desc &d = lens[i];
-        if ((e = cudaMemcpy(ix->bA + (uint64_t)i * nbins, d.bA, sizeof(uint32_t) * nbins, cudaMemcpyHostToDevice)) !=
-            cudaSuccess)
-            return cleanup(cuda_fail(e, "gx_index_upload bA"));
-        if (d.npep) {
-            if ((e = cudaMemcpy(ix->iA + hl[i].ia_off, d.iA, sizeof(uint32_t) * (uint64_t)d.npep * d.speclen,
-                                cudaMemcpyHostToDevice)) != cudaSuccess)
-                return cleanup(cuda_fail(e, "gx_index_upload iA"));
-            if ((e = cudaMemcpy(ix->mass + hl[i].mass_off, d.mass, sizeof(float) * d.npep, cudaMemcpyHostToDevice)) !=
-                cudaSuccess)
-                return cleanup(cuda_fail(e, "gx_index_upload mass"));
-            const uint64_t nid = (uint64_t)d.npep * d.speclen;
-            k_encode_ids<<<(unsigned)std::min<uint64_t>((nid + 255) / 256, 65535), 256>>>(ix->iA + hl[i].ia_off, nid,
-                                                                                        d.speclen, d.speclen / 2,
-                                                                                        hl[i].magic);
-            count_launch();
-            if ((e = cudaGetLastError()) != cudaSuccess) return cleanup(cuda_fail(e, "gx_index_upload encode"));
-        }
-    }
-    if ((e = cudaMemcpy(ix->lens, hl.data(), sizeof(DevLen) * nlen, cudaMemcpyHostToDevice)) != cudaSuccess)
-        return cleanup(cuda_fail(e, "gx_index_upload lens"));
-    if ((e = cudaDeviceSynchronize()) != cudaSuccess) return cleanup(cuda_fail(e, "gx_index_upload"));
-    *out = ix;
-    return GX_SUCCESS;
-}
 
-extern "C" gx_status gx_index_free(gx_index *ix)
-{
-    if (!ix) return GX_SUCCESS;
-    cudaSetDevice(ix->device);
-    cudaFree(ix->bA);
-    cudaFree(ix->iA);
-    cudaFree(ix->mass);
-    cudaFree(ix->lens);
-    delete ix;
-    return GX_SUCCESS;
-}
-
-extern "C" uint64_t gx_index_bytes(const gx_index *ix) { return ix ? ix->bytes : 0; }
 
 extern "C" gx_status gx_workspace_free(gx_workspace *ws)
 {
@@ -666,7 +556,7 @@ gx_status launch_search(gx_index *ix, gx_workspace *ws, const gx_queries *q, con
     if (q->nspec > ws->max_spec) return fail(GX_ERR_INVLD_SIZE, "more spectra than the workspace holds");
     if (q->nspec == 0) return GX_SUCCESS;
     SearchArgs a{};
-    a.bA = ix->bA; a.iA = ix->iA; a.mass = ix->mass; a.lens = ix->lens; a.nlen = ix->nlen; a.nbins = ix->nbins;
+    a.bA = ix->bA; a.iA = ix->iA; a.iAb = ix->iAb; a.blkA = ix->blkA; a.block = ix->block; a.mass = ix->mass; a.lens = ix->lens; a.nlen = ix->nlen; a.nbins = ix->nbins;
     a.maxz = ix->maxz;
     a.qidx = q->idx; a.moz = q->moz; a.intn = q->intn; a.prec = q->prec; a.dMq = q->dM; a.nspec = q->nspec;
     a.dM = p->dM;
