@@ -168,8 +168,9 @@ constexpr int kBBlock = 1024;
 constexpr int kBWarps = kBBlock / 32;
 constexpr int kPend = 64;       // per-warp queue of candidates awaiting a hyperscore
 constexpr int kIvlChunk = 1024; // intervals per span table
-constexpr int kUnit = 1024;     // ids per warp work unit (32 per lane)
+constexpr int kUnit = 256;      // ids per warp work unit
 constexpr int kIlp = 8;         // iA loads in flight per lane
+constexpr int kEntSmem = 4;     // heap entrants per warp kept in shared memory
 
 // Dynamic shared memory after the scorecard tile:
 //   queued candidates a = packed word (or wide counts | b-sum << 32),
@@ -210,6 +211,7 @@ struct BatchSmem {
 
     uint32_t scan_tmp[kBWarps];
     int32_t warp_cnt[kBWarps];
+    Cell ent_s[kBWarps][kEntSmem];   // first heap entrants of each warp (the rest spill to global)
     int32_t heap_size;
     int32_t cpsms;
     int32_t status;
@@ -266,8 +268,11 @@ __device__ __forceinline__ void score_queue(BatchSmem &sm, const BatchDyn &dd, c
             yi = min(yi, 80u);
         }
         const double h1 = sm.lgf[bi] + sm.lgf[yi];
-        float h = __double2float_rn(h1 + log10((double)(uint32_t)(1u + ib)) + log10((double)(uint32_t)(1u + iy)) -
-                                    4.0);
+        const uint32_t xb = 1u + ib, xy = 1u + iy;
+        // log10 of small integers from a table filled by the same log10 (identical values)
+        const double lb = xb < a.logtab_n ? __ldg(a.logtab + xb) : log10((double)xb);
+        const double ly = xy < a.logtab_n ? __ldg(a.logtab + xy) : log10((double)xy);
+        float h = __double2float_rn(h1 + lb + ly - 4.0);
         if (h > 0.0f) {
             if (h >= 80.0f) h = 79.0f;
             psm = true;
@@ -285,8 +290,47 @@ __device__ __forceinline__ void score_queue(BatchSmem &sm, const BatchDyn &dd, c
     cps += __popc(pb);
     const bool e = psm && cell.h >= tau;
     const unsigned eb = __ballot_sync(0xffffffffu, e);
-    if (e) ent[nent + __popc(eb & ((1u << lane) - 1u))] = cell;
+    if (e) {
+        const int g = nent + __popc(eb & ((1u << lane) - 1u));
+        if (g < kEntSmem) sm.ent_s[wid][g] = cell;
+        else ent[g] = cell;
+    }
     nent += __popc(eb);
+}
+
+// Out-of-line heap insertion (keeps the persistent kernel's register budget for the
+// streaming loop).
+__device__ __noinline__ void heap_insert_many(Cell *heap, int *size, int cap, const Cell *cells, int n)
+{
+    int hs = *size;
+    for (int k = 0; k < n; k++) heap_insert(heap, hs, cap, cells[k]);
+    *size = hs;
+}
+
+// Thread 0 inserts the entrants of warps 0..31 of the last scanned tile, in order: the
+// first few of each warp from shared memory, any overflow from the warp's global spill.
+__device__ __noinline__ void insert_entrants(BatchSmem &sm, const Cell *spill_cta, uint32_t spill_per_warp, int cap)
+{
+    int hs = sm.heap_size;
+    for (int w2 = 0; w2 < kBWarps; w2++) {
+        const int n2 = sm.warp_cnt[w2];
+        const int ns = min(n2, kEntSmem);
+        for (int k = 0; k < ns; k++) heap_insert(sm.heap, hs, cap, sm.ent_s[w2][k]);
+        if (n2 > kEntSmem) {
+            sm.heap_size = hs;
+            const Cell *e2 = spill_cta + (uint64_t)w2 * spill_per_warp;
+            for (int k0 = kEntSmem; k0 < n2; k0 += 8) {
+                Cell c8[8];
+#pragma unroll
+                for (int k = 0; k < 8; k++)
+                    if (k0 + k < n2) c8[k] = e2[k0 + k];
+                heap_insert_many(sm.heap, &sm.heap_size, cap, c8, min(8, n2 - k0));
+            }
+            hs = sm.heap_size;
+        }
+    }
+    sm.heap_size = hs;
+    sm.root = sm.heap[0].h;
 }
 
 // Span table of up to kIvlChunk intervals for one length: iA start of each interval's
@@ -374,6 +418,7 @@ __global__ void __launch_bounds__(kBBlock, 1) k_search_batched(SearchArgs a)
         const uint32_t nv = a.nivl[s];
         const Interval *ivl = a.ivl + 2ull * a.qidx[s];
         int cps = 0;   // candidate PSMs counted by this warp (lane 0 adds them at the end)
+        bool heap_due = false;
 
         for (int ixx = 0; ixx < a.nlen; ixx++) {
             const int2 w = a.win[(uint64_t)s * a.nlen + ixx];
@@ -401,6 +446,10 @@ __global__ void __launch_bounds__(kBBlock, 1) k_search_batched(SearchArgs a)
                         build_span_table(sm, dd, ivl + ic0, ncv, bA, tid, lane, wid);
                     if (tid == 0) sm.next_unit = 0;
                     __syncthreads();
+                    if (heap_due) {          // the previous tile's entrants, off the critical path
+                        if (tid == 0) insert_entrants(sm, a.spill + (uint64_t)blockIdx.x * kBWarps * a.spill_per_warp, a.spill_per_warp, a.heap_cap);
+                        heap_due = false;
+                    }
                     const uint32_t M = dd.sp_pre[ncv];
                     for (;;) {
                         uint32_t u = 0;
@@ -445,69 +494,122 @@ __global__ void __launch_bounds__(kBBlock, 1) k_search_batched(SearchArgs a)
                 }
                 // ---- scan: each warp owns a contiguous range, in entry order ------------
                 const float tau = sm.heap_size < a.heap_cap ? -1.0f : sm.root;
-                const int R = (tn + kBWarps - 1) / kBWarps;
+                const int R = (((tn + kBWarps - 1) / kBWarps) + 3) & ~3;   // multiple of 4
                 const int r0 = min(tn, wid * R), r1 = min(tn, r0 + R);
                 int npend = 0, nent = 0;
-                for (int base = r0; base < r1; base += 32) {
-                    const int c = base + lane;
-                    bool is = false;
-                    unsigned long long va = 0ull, vb = 0ull;
-                    if (c < r1) {
-                        uint32_t bc, yc;
-                        if (!wide) {
-                            const uint32_t wb = scp[c], wy = scp[T + c];
-                            scp[c] = 0u;
-                            scp[T + c] = 0u;
-                            va = (unsigned long long)wb | ((unsigned long long)wy << 32);
-                            bc = wb >> 24;
-                            yc = wy >> 24;
-                            vb = (uint32_t)c;
-                        } else {
+                if (!wide) {
+                    // four candidates per lane (128-bit shared loads and stores), appended to the
+                    // queue in candidate order through a warp scan of per-lane counts
+                    for (int base = r0; base < r1; base += 128) {
+                        const int c4 = base + 4 * lane;
+                        uint4 wb = make_uint4(0, 0, 0, 0), wy = make_uint4(0, 0, 0, 0);
+                        if (c4 < r1) {
+                            wb = *reinterpret_cast<const uint4 *>(scp + c4);
+                            wy = *reinterpret_cast<const uint4 *>(scp + T + c4);
+                        }
+                        const uint32_t minshp = a.min_shp;
+                        const unsigned m = ((((wb.x >> 24) + (wy.x >> 24)) & 0xFFFFu) >= minshp ? 1u : 0u) |
+                                           ((((wb.y >> 24) + (wy.y >> 24)) & 0xFFFFu) >= minshp ? 2u : 0u) |
+                                           ((((wb.z >> 24) + (wy.z >> 24)) & 0xFFFFu) >= minshp ? 4u : 0u) |
+                                           ((((wb.w >> 24) + (wy.w >> 24)) & 0xFFFFu) >= minshp ? 8u : 0u);
+                        const int cnt = __popc(m);
+                        int incl = cnt;
+#pragma unroll
+                        for (int o = 1; o < 32; o <<= 1) {
+                            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                            if (lane >= o) incl += y;
+                        }
+                        const int total = __shfl_sync(0xffffffffu, incl, 31);
+                        if (c4 < r1 && m) {   // words of entries without a PSM are zeroed here, the rest below
+                            *reinterpret_cast<uint4 *>(scp + c4) = make_uint4(0, 0, 0, 0);
+                            *reinterpret_cast<uint4 *>(scp + T + c4) = make_uint4(0, 0, 0, 0);
+                        } else if (c4 < r1 && (wb.x | wb.y | wb.z | wb.w | wy.x | wy.y | wy.z | wy.w)) {
+                            *reinterpret_cast<uint4 *>(scp + c4) = make_uint4(0, 0, 0, 0);
+                            *reinterpret_cast<uint4 *>(scp + T + c4) = make_uint4(0, 0, 0, 0);
+                        }
+                        if (total == 0) continue;
+                        const int excl = incl - cnt;
+                        int done = 0;
+                        while (done < total) {
+                            const int room = kPend - npend;
+                            int r = 0;
+                            auto put1 = [&](unsigned bit, uint32_t b, uint32_t y, int j) {
+                                if (m & bit) {
+                                    const int g = excl + r;
+                                    if (g >= done && g < done + room) {
+                                        const int slot = npend + (g - done);
+                                        dd.pend_a[wid][slot] = (unsigned long long)b | ((unsigned long long)y << 32);
+                                        dd.pend_b[wid][slot] = (unsigned long long)(uint32_t)(c4 + j);
+                                    }
+                                    r++;
+                                }
+                            };
+                            put1(1u, wb.x, wy.x, 0);
+                            put1(2u, wb.y, wy.y, 1);
+                            put1(4u, wb.z, wy.z, 2);
+                            put1(8u, wb.w, wy.w, 3);
+                            const int put = min(room, total - done);
+                            npend += put;
+                            done += put;
+                            __syncwarp();
+                            while (npend >= 32) {
+                                score_queue(sm, dd, a, wid, lane, 32, t0, ixx, speclen, tau, wide, ent, nent, cps);
+                                __syncwarp();
+                                const unsigned long long ka = lane + 32 < npend ? dd.pend_a[wid][32 + lane] : 0ull;
+                                const unsigned long long kb = lane + 32 < npend ? dd.pend_b[wid][32 + lane] : 0ull;
+                                __syncwarp();
+                                if (lane + 32 < npend) {
+                                    dd.pend_a[wid][lane] = ka;
+                                    dd.pend_b[wid][lane] = kb;
+                                }
+                                npend -= 32;
+                                __syncwarp();
+                            }
+                        }
+                    }
+                } else {
+                    for (int base = r0; base < r1; base += 32) {
+                        const int c = base + lane;
+                        bool is = false;
+                        unsigned long long va = 0ull, vb = 0ull;
+                        if (c < r1) {
                             const uint32_t cnt = scw_cnt[c];
-                            bc = cnt & 0xFFFFu;
-                            yc = cnt >> 16;
+                            const uint32_t bc = cnt & 0xFFFFu, yc = cnt >> 16;
                             va = (unsigned long long)cnt | ((unsigned long long)scw_ib[c] << 32);
                             vb = (unsigned long long)(uint32_t)c | ((unsigned long long)scw_iy[c] << 32);
                             scw_cnt[c] = 0; scw_ib[c] = 0; scw_iy[c] = 0;
+                            is = ((bc + yc) & 0xFFFFu) >= a.min_shp;
                         }
-                        is = ((bc + yc) & 0xFFFFu) >= a.min_shp;
-                    }
-                    const unsigned bal = __ballot_sync(0xffffffffu, is);
-                    if (is) {
-                        const int slot = npend + __popc(bal & ((1u << lane) - 1u));
-                        dd.pend_a[wid][slot] = va;
-                        dd.pend_b[wid][slot] = vb;
-                    }
-                    npend += __popc(bal);
-                    __syncwarp();
-                    if (npend >= 32) {
-                        score_queue(sm, dd, a, wid, lane, 32, t0, ixx, speclen, tau, wide, ent, nent, cps);
-                        __syncwarp();
-                        if (lane < npend - 32) {
-                            dd.pend_a[wid][lane] = dd.pend_a[wid][32 + lane];
-                            dd.pend_b[wid][lane] = dd.pend_b[wid][32 + lane];
+                        const unsigned bal = __ballot_sync(0xffffffffu, is);
+                        if (is) {
+                            const int slot = npend + __popc(bal & ((1u << lane) - 1u));
+                            dd.pend_a[wid][slot] = va;
+                            dd.pend_b[wid][slot] = vb;
                         }
-                        npend -= 32;
+                        npend += __popc(bal);
                         __syncwarp();
+                        if (npend >= 32) {
+                            score_queue(sm, dd, a, wid, lane, 32, t0, ixx, speclen, tau, wide, ent, nent, cps);
+                            __syncwarp();
+                            if (lane < npend - 32) {
+                                dd.pend_a[wid][lane] = dd.pend_a[wid][32 + lane];
+                                dd.pend_b[wid][lane] = dd.pend_b[wid][32 + lane];
+                            }
+                            npend -= 32;
+                            __syncwarp();
+                        }
                     }
                 }
                 if (npend > 0) score_queue(sm, dd, a, wid, lane, npend, t0, ixx, speclen, tau, wide, ent, nent, cps);
                 if (lane == 0) sm.warp_cnt[wid] = nent;
                 __syncthreads();
                 // ---- exact heap: entrants of all warps, in entry order ------------------
-                if (tid == 0) {
-                    int hs = sm.heap_size;
-                    for (int w2 = 0; w2 < kBWarps; w2++) {
-                        const Cell *e2 = a.spill + ((uint64_t)blockIdx.x * kBWarps + w2) * (uint64_t)a.spill_per_warp;
-                        const int n2 = sm.warp_cnt[w2];
-                        for (int k = 0; k < n2; k++) heap_insert(sm.heap, hs, a.heap_cap, e2[k]);
-                    }
-                    sm.heap_size = hs;
-                    sm.root = sm.heap[0].h;
-                }
+                heap_due = true;   // inserted by thread 0 while the next tile streams
               }
             }
         }
+        if (heap_due && tid == 0)
+            insert_entrants(sm, a.spill + (uint64_t)blockIdx.x * kBWarps * a.spill_per_warp, a.spill_per_warp, a.heap_cap);
         if (lane == 0 && cps) atomicAdd(&sm.cpsms, cps);
         __syncthreads();
         // ---- per-spectrum outputs (the tail fit runs in k_tailfit) -------------------
@@ -571,6 +673,19 @@ size_t batched_sort_temp_bytes(uint32_t max_spec)
     cub::DeviceRadixSort::SortPairsDescending(nullptr, bytes, (const uint64_t *)nullptr, (uint64_t *)nullptr,
                                               (const uint32_t *)nullptr, (uint32_t *)nullptr, (int)max_spec);
     return bytes;
+}
+
+__global__ void k_logtab(double *tab, uint32_t n)
+{
+    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x < n) tab[x] = log10((double)x);
+}
+
+cudaError_t fill_logtab(double *tab, uint32_t n, cudaStream_t st)
+{
+    k_logtab<<<(n + 255) / 256, 256, 0, st>>>(tab, n);
+    count_launch();
+    return cudaGetLastError();
 }
 
 size_t batched_dyn_smem(int tile) { return (size_t)tile * 8 + batch_dyn_bytes(); }

@@ -19,6 +19,9 @@ struct BatchedScratch {
 };
 
 size_t batched_sort_temp_bytes(uint32_t max_spec);
+// log10(x) for x in [0, n), computed on the device by the function the kernels call
+cudaError_t fill_logtab(double *tab, uint32_t n, cudaStream_t st);
+constexpr uint32_t kLogTab = 1u << 20;
 cudaError_t batched_set_attributes(int tile);
 cudaError_t launch_batched(SearchArgs a, const BatchedScratch &b, cudaStream_t st);
 

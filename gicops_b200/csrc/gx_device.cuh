@@ -79,6 +79,8 @@ struct SearchArgs {
     double expect_max;
     uint32_t flags;
     const double *lgfact; // [81]
+    const double *logtab; // [logtab_n]: log10(x) for small integers x
+    uint32_t logtab_n;
     // scratch / outputs
     const int2 *win;      // [nspec * nlen] candidate window per (spectrum, length)
     // batched path

@@ -389,6 +389,7 @@ struct gx_workspace {
     uint32_t *nivl = nullptr, *guard = nullptr, *queue = nullptr, *hist_g = nullptr;
     Cell *spill = nullptr;
     uint32_t spill_per_warp = 0;
+    double *logtab = nullptr;
     BatchedScratch bs{};
     int tile = kBlockEntries;
 };
@@ -452,7 +453,7 @@ extern "C" gx_status gx_workspace_free(gx_workspace *ws)
     if (ws->ix) cudaSetDevice(ws->ix->device);
     void *ptrs[] = {ws->win, ws->lgfact, ws->err, ws->qidx, ws->moz, ws->intn, ws->charge, ws->prec,
                     ws->dMq, ws->out, ws->heap, ws->hist, ws->ivl, ws->nivl, ws->guard, ws->queue,
-                    ws->hist_g, ws->spill, ws->bs.key_in, ws->bs.key_out, ws->bs.ord_in, ws->bs.ord_out, ws->bs.sort_temp};
+                    ws->hist_g, ws->spill, ws->logtab, ws->bs.key_in, ws->bs.key_out, ws->bs.ord_in, ws->bs.ord_out, ws->bs.sort_temp};
     for (void *p : ptrs) cudaFree(p);
     if (ws->stream) cudaStreamDestroy(ws->stream);
     delete ws;
@@ -504,6 +505,9 @@ extern "C" gx_status gx_workspace_create(const gx_index *ix, uint32_t max_spec, 
     }
     ws->spill_per_warp = (uint32_t)((ws->tile + 31) / 32);
     al((void **)&ws->spill, sizeof(Cell) * (uint64_t)ws->bs.grid * 32 * ws->spill_per_warp);
+    al((void **)&ws->logtab, sizeof(double) * kLogTab);
+    if (e == cudaSuccess) e = fill_logtab(ws->logtab, kLogTab, nullptr);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e == cudaSuccess) e = batched_set_attributes(ws->tile);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
@@ -571,6 +575,8 @@ gx_status launch_search(gx_index *ix, gx_workspace *ws, const gx_queries *q, con
         a.hist_g = hist ? hist : ws->hist_g;
         a.tile = ws->tile;
         a.spill = ws->spill;
+        a.logtab = ws->logtab;
+        a.logtab_n = kLogTab;
         a.spill_per_warp = ws->spill_per_warp;
         cudaError_t e = launch_batched(a, ws->bs, st);
         if (e != cudaSuccess) return cuda_fail(e, "batched search launch");
