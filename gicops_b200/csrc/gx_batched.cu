@@ -307,6 +307,21 @@ __device__ __noinline__ void heap_insert_many(Cell *heap, int *size, int cap, co
     *size = hs;
 }
 
+// Bring iA span [st, en) of a block into L2 ahead of its tile: one bulk prefetch per span,
+// rounded out to 16-byte boundaries inside the iAb allocation.
+__device__ __forceinline__ void prefetch_span(const uint32_t *iAb_base, uint64_t iab_bytes, const uint32_t *iA,
+                                              uint32_t st, uint32_t en)
+{
+    if (en <= st) return;
+    const uint64_t base = reinterpret_cast<uint64_t>(iAb_base);
+    uint64_t lo = reinterpret_cast<uint64_t>(iA + st) & ~15ull;
+    uint64_t hi = (reinterpret_cast<uint64_t>(iA + en) + 15ull) & ~15ull;
+    const uint64_t end = (base + iab_bytes) & ~15ull;
+    if (hi > end) hi = end;
+    if (lo < base || hi <= lo) return;
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(lo), "r"((uint32_t)(hi - lo)) : "memory");
+}
+
 // Thread 0 inserts the entrants of warps 0..31 of the last scanned tile, in order: the
 // first few of each warp from shared memory, any overflow from the warp's global spill.
 __device__ __noinline__ void insert_entrants(BatchSmem &sm, const Cell *spill_cta, uint32_t spill_per_warp, int cap)
@@ -450,6 +465,34 @@ __global__ void __launch_bounds__(kBBlock, 1) k_search_batched(SearchArgs a)
                         if (tid == 0) insert_entrants(sm, a.spill + (uint64_t)blockIdx.x * kBWarps * a.spill_per_warp, a.spill_per_warp, a.heap_cap);
                         heap_due = false;
                     }
+                    if (ic0 == 0 && ti + 1 == nsub) {
+                        // the next tile of this spectrum: the next block of this length, or the
+                        // first block of the next length with a window; prefetch its spans into L2
+                        int nx = -1;
+                        int64_t nkb = 0;
+                        if (kb < kb1) {
+                            nx = ixx;
+                            nkb = kb + 1;
+                        } else {
+                            for (int j = ixx + 1; j < a.nlen; j++) {
+                                const int2 w2 = a.win[(uint64_t)s * a.nlen + j];
+                                if (w2.y >= w2.x) {
+                                    nx = j;
+                                    nkb = w2.x / E;
+                                    break;
+                                }
+                            }
+                        }
+                        if (nx >= 0) {
+                            const DevLen nl = a.lens[nx];
+                            const uint32_t *nbA = a.blkA + nl.blk_off + (uint64_t)nkb * (a.nbins + 1);
+                            const uint32_t *niA = a.iAb + nl.ia_off;
+                            for (uint32_t i = tid; i < nv; i += kBBlock) {
+                                const Interval v = ivl[i];
+                                prefetch_span(a.iAb, a.iab_bytes, niA, __ldg(nbA + v.b0), __ldg(nbA + v.b1 + 1));
+                            }
+                        }
+                    }
                     const uint32_t M = dd.sp_pre[ncv];
                     for (;;) {
                         uint32_t u = 0;
@@ -464,30 +507,41 @@ __global__ void __launch_bounds__(kBBlock, 1) k_search_batched(SearchArgs a)
                             const uint32_t mid = (lo + hi) >> 1;
                             if (dd.sp_pre[mid] <= f0) lo = mid; else hi = mid;
                         }
-                        // walk the unit interval by interval: bookkeeping once per interval
+                        // walk the unit in windows of 8 x 32 flat positions; a window spans at most
+                        // two consecutive intervals (it stops where a third one would begin)
                         uint32_t k = lo, f = f0;
                         while (f < f1) {
-                            const uint32_t fe = min(f1, dd.sp_pre[k + 1]);
-                            const uint32_t delta = dd.sp_start[k] - dd.sp_pre[k];   // iA index = flat + delta (mod 2^32)
-                            const uint2 cs = dd.sp_cs[k];
+                            while (dd.sp_pre[k + 1] <= f) k++;
+                            const uint32_t p1 = dd.sp_pre[k + 1];                 // start of interval k+1
+                            const uint32_t p2 = k + 2 <= ncv ? dd.sp_pre[min(k + 2, ncv)] : p1;
+                            const uint32_t lim = min(min(f1, f + 32u * kIlp), max(p1, p2));
+                            const uint32_t d0 = dd.sp_start[k] - dd.sp_pre[k];
+                            const uint2 c0 = dd.sp_cs[k];
+                            const bool two = k + 1 < ncv;
+                            const uint32_t d1 = two ? dd.sp_start[k + 1] - p1 : d0;
+                            const uint2 c1 = two ? dd.sp_cs[k + 1] : c0;
                             if (!wide) {
-                                const uint32_t vb = (cs.y << 24) | cs.x;
-                                for (uint32_t g = f + lane; g < fe; g += 32 * kIlp) {
-                                    uint32_t idv[kIlp];
+                                const uint32_t v0 = (c0.y << 24) | c0.x, v1 = (c1.y << 24) | c1.x;
+                                uint32_t idv[kIlp], vv[kIlp];
 #pragma unroll
-                                    for (int j = 0; j < kIlp; j++)
-                                        idv[j] = (g + 32u * j < fe) ? __ldg(iA + (g + 32u * j + delta)) : idlo - 1u;
-#pragma unroll
-                                    for (int j = 0; j < kIlp; j++)
-                                        scatter_packed(scp, idv[j], idlo, span, (uint32_t)T, vb);
+                                for (int j = 0; j < kIlp; j++) {
+                                    const uint32_t g = f + lane + 32u * j;
+                                    const bool in1 = g >= p1;
+                                    vv[j] = in1 ? v1 : v0;
+                                    idv[j] = g < lim ? __ldg(iA + (g + (in1 ? d1 : d0))) : idlo - 1u;
                                 }
+#pragma unroll
+                                for (int j = 0; j < kIlp; j++)
+                                    scatter_packed(scp, idv[j], idlo, span, (uint32_t)T, vv[j]);
                             } else {
-                                for (uint32_t g = f + lane; g < fe; g += 32)
-                                    scatter_wide(scw_cnt, scw_ib, scw_iy, __ldg(iA + (g + delta)), idlo, span, cs.y,
-                                                 cs.x);
+                                for (uint32_t g = f + lane; g < lim; g += 32) {
+                                    const bool in1 = g >= p1;
+                                    const uint2 c = in1 ? c1 : c0;
+                                    scatter_wide(scw_cnt, scw_ib, scw_iy, __ldg(iA + (g + (in1 ? d1 : d0))), idlo, span,
+                                                 c.y, c.x);
+                                }
                             }
-                            f = fe;
-                            k++;
+                            f = lim;
                         }
                     }
                     __syncthreads();
@@ -512,42 +566,33 @@ __global__ void __launch_bounds__(kBBlock, 1) k_search_batched(SearchArgs a)
                                            ((((wb.y >> 24) + (wy.y >> 24)) & 0xFFFFu) >= minshp ? 2u : 0u) |
                                            ((((wb.z >> 24) + (wy.z >> 24)) & 0xFFFFu) >= minshp ? 4u : 0u) |
                                            ((((wb.w >> 24) + (wy.w >> 24)) & 0xFFFFu) >= minshp ? 8u : 0u);
-                        const int cnt = __popc(m);
-                        int incl = cnt;
-#pragma unroll
-                        for (int o = 1; o < 32; o <<= 1) {
-                            const int y = __shfl_up_sync(0xffffffffu, incl, o);
-                            if (lane >= o) incl += y;
-                        }
-                        const int total = __shfl_sync(0xffffffffu, incl, 31);
-                        if (c4 < r1 && m) {   // words of entries without a PSM are zeroed here, the rest below
-                            *reinterpret_cast<uint4 *>(scp + c4) = make_uint4(0, 0, 0, 0);
-                            *reinterpret_cast<uint4 *>(scp + T + c4) = make_uint4(0, 0, 0, 0);
-                        } else if (c4 < r1 && (wb.x | wb.y | wb.z | wb.w | wy.x | wy.y | wy.z | wy.w)) {
+                        // order of queued entries: lane-major, bit order inside a lane
+                        const unsigned lt = (1u << lane) - 1u;
+                        const unsigned b0 = __ballot_sync(0xffffffffu, m & 1u), b1 = __ballot_sync(0xffffffffu, m & 2u);
+                        const unsigned b2 = __ballot_sync(0xffffffffu, m & 4u), b3 = __ballot_sync(0xffffffffu, m & 8u);
+                        const int total = __popc(b0) + __popc(b1) + __popc(b2) + __popc(b3);
+                        if (c4 < r1 && (wb.x | wb.y | wb.z | wb.w | wy.x | wy.y | wy.z | wy.w)) {
                             *reinterpret_cast<uint4 *>(scp + c4) = make_uint4(0, 0, 0, 0);
                             *reinterpret_cast<uint4 *>(scp + T + c4) = make_uint4(0, 0, 0, 0);
                         }
                         if (total == 0) continue;
-                        const int excl = incl - cnt;
+                        const int excl = __popc(b0 & lt) + __popc(b1 & lt) + __popc(b2 & lt) + __popc(b3 & lt);
                         int done = 0;
                         while (done < total) {
                             const int room = kPend - npend;
                             int r = 0;
-                            auto put1 = [&](unsigned bit, uint32_t b, uint32_t y, int j) {
-                                if (m & bit) {
-                                    const int g = excl + r;
-                                    if (g >= done && g < done + room) {
-                                        const int slot = npend + (g - done);
-                                        dd.pend_a[wid][slot] = (unsigned long long)b | ((unsigned long long)y << 32);
-                                        dd.pend_b[wid][slot] = (unsigned long long)(uint32_t)(c4 + j);
-                                    }
-                                    r++;
+                            for (unsigned mm = m; mm; mm &= mm - 1u) {
+                                const int j = __ffs(mm) - 1;
+                                const int g = excl + r;
+                                if (g >= done && g < done + room) {
+                                    const uint32_t bj = j == 0 ? wb.x : j == 1 ? wb.y : j == 2 ? wb.z : wb.w;
+                                    const uint32_t yj = j == 0 ? wy.x : j == 1 ? wy.y : j == 2 ? wy.z : wy.w;
+                                    const int slot = npend + (g - done);
+                                    dd.pend_a[wid][slot] = (unsigned long long)bj | ((unsigned long long)yj << 32);
+                                    dd.pend_b[wid][slot] = (unsigned long long)(uint32_t)(c4 + j);
                                 }
-                            };
-                            put1(1u, wb.x, wy.x, 0);
-                            put1(2u, wb.y, wy.y, 1);
-                            put1(4u, wb.z, wy.z, 2);
-                            put1(8u, wb.w, wy.w, 3);
+                                r++;
+                            }
                             const int put = min(room, total - done);
                             npend += put;
                             done += put;

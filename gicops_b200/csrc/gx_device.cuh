@@ -57,6 +57,7 @@ struct SearchArgs {
     const uint32_t *iAb;  // block layout: per block of `block` entries, a CSR over bins
     const uint32_t *blkA; // block layout offsets [nblk][nbins + 1] per length (relative to ia_off)
     uint32_t block;       // entries per block
+    uint64_t iab_bytes;   // size of iAb (bounds the L2 prefetches)
     const float *mass;
     const DevLen *lens;
     int32_t nlen;
