@@ -142,6 +142,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain", action="store_true", help="time the plain one-spectrum-per-CTA path instead")
     ap.add_argument("--compare-plain", action="store_true", help="also time one step of the plain path")
+    ap.add_argument("--spectra", type=int, default=0, help="search only the first N spectra (profiling cases)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -180,6 +181,8 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
 
     w, db, H, q = make_workload(args.workload, rank)
+    if args.spectra:
+        q = q.subset(np.arange(min(args.spectra, q.n)))
     params = gx.SearchParams(dM=w["dM"], dF=5, topmatches=5, expect_max=20.0,
                              flags=gx.FLAG_PLAIN if args.plain else 0)
     dev = gx.DeviceIndex(H, local)
@@ -308,7 +311,8 @@ def main():
             "metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int32+f64", "data": "synthetic (seeded generator, no dataset)",
-            "config": {"workload": args.workload, "spectra_per_gpu": q.n, "proteins": w["nproteins"],
+            "config": {"workload": args.workload + (f" (first {q.n} spectra)" if args.spectra else ""),
+                       "spectra_per_gpu": q.n, "proteins": w["nproteins"],
                        "index_entries": H.total_entries(), "index_ion_ids": H.total_ions(),
                        "window_da": w["dM"], "frag_tol_bins": 5, "topK": 5,
                        "l2": "inputs larger than L2 (index %.2f GB)" % (dev.nbytes / 1e9),
