@@ -17,6 +17,7 @@ LIB_PATH = os.path.join(HERE, "_lib", "libgicops_b200.so")
 HIST_BINS = 802
 MAX_HEAP = 31
 MAX_PEAKS = 1024
+NOALLOC_MAX_WINDOWS = 1 << 19
 
 SUCCESS = 0
 STATUS_NAMES = {
@@ -100,6 +101,8 @@ _SIGS = [
                                    C.c_void_p, C.c_void_p]),
     ("gx_search_device", C.c_int32, [C.c_void_p, C.c_void_p, C.POINTER(Queries), C.POINTER(Params), C.c_void_p,
                                      C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("gx_search_device_noalloc", C.c_int32, [C.c_void_p, C.POINTER(Queries), C.POINTER(Params), C.c_void_p,
+                                             C.c_void_p, C.c_void_p, C.c_void_p]),
     ("gx_traffic_host", C.c_int32, [C.POINTER(LengthDesc), C.c_int32, C.POINTER(Queries), C.POINTER(Params),
                                     C.c_void_p, C.c_void_p, C.c_int32]),
     ("gx_heap_capacity", C.c_int32, [C.c_uint32]),

@@ -180,6 +180,21 @@ gx_status gx_search_host(gx_index *ix, gx_workspace *ws, const gx_queries *q, co
 gx_status gx_search_device(gx_index *ix, gx_workspace *ws, const gx_queries *q_dev, const gx_params *p,
                            gx_result *out_dev, gx_cell *heap_dev, uint32_t *hist_dev, void *stream);
 
+/* Search with DEVICE buffers and no device allocation of any kind (no counterpart in
+ * the reference).  For callers that cannot call cudaMalloc: hosts whose memory pool owns
+ * every byte of the device, callers with a memory budget fixed at start-up, or code where
+ * an allocation could block or fail at an unsafe point.  It runs the plain path
+ * (GX_FLAG_PLAIN semantics) with its scratch in a fixed file-scope device array of
+ * GX_NOALLOC_MAX_WINDOWS windows (4 MiB, held by every device that loads the library until
+ * exit); batches with nspec * nlen above that are rejected with GX_ERR_INVLD_SIZE.  The
+ * first call on a device looks the array up and sets the kernel up on that device: make
+ * it before any stream capture.  All calls share the array; calls that overlap on the GPU
+ * race and must be serialised by the caller.  Stream-ordered, no synchronisation; the
+ * device guard word (too many peaks) is not reported. */
+#define GX_NOALLOC_MAX_WINDOWS (1u << 19)
+gx_status gx_search_device_noalloc(gx_index *ix, const gx_queries *q_dev, const gx_params *p, gx_result *out_dev,
+                                   gx_cell *heap_dev, uint32_t *hist_dev, void *stream);
+
 /* Algorithmic traffic of the path, per spectrum (host arrays, for roofline figures):
  * ids_out[s] = ion ids inside the precursor window of every distinct probed bin,
  * bins_out[s] = distinct probed bins, both summed over lengths with a non-empty

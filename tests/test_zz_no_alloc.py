@@ -1,0 +1,93 @@
+"""gx_search_device_noalloc: the query path for callers that cannot allocate device memory
+(a host whose memory pool owns the whole device, a fixed start-up memory budget, or code
+where an allocation could block or fail at a bad moment).  It keeps its scratch in a
+fixed-size array inside the library instead of a workspace.
+
+Checked here through the C ABI: two calls in a row give the same results as the
+allocating entry point (the array keeps the previous call's contents, so the second call
+shows that nothing stale leaks through), and batches beyond the array's size are refused.
+This file is named so that pytest collects it last.
+"""
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from conftest import has_gpu, search_params
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev_queries(q, torch, N):
+    d = torch.device("cuda", 0)
+    t = dict(idx=torch.from_numpy(q.idx.view(np.int32).copy()).to(d), moz=torch.from_numpy(q.moz.copy()).to(d),
+             intn=torch.from_numpy(q.intn.copy()).to(d), prec=torch.from_numpy(q.prec.copy()).to(d))
+    cq = N.Queries(q.n, len(q.moz), t["idx"].data_ptr(), t["moz"].data_ptr(), t["intn"].data_ptr(),
+                   t["prec"].data_ptr(), None, None)
+    return cq, t
+
+
+def test_noalloc_matches_allocating_path(golden):
+    if not has_gpu():
+        pytest.skip("no CUDA device")
+    import torch
+    import gicops_b200 as gx
+    import gicops_b200._native as N
+
+    c = golden("open_mox")
+    H, q = c["index"], c["queries"]
+    dev = gx.DeviceIndex(H, 0)
+    ws = gx.Searcher(dev, q.n, len(q.moz))
+    p = search_params(c, flags=gx.FLAG_PLAIN)
+    cap = p.heap_cap
+    cq, keep = _dev_queries(q, torch, N)
+    cp = p.c()
+    d = torch.device("cuda", 0)
+
+    def outputs():
+        return (torch.zeros(q.n * N.RESULT_DTYPE.itemsize, dtype=torch.uint8, device=d),
+                torch.zeros(q.n * cap * N.CELL_DTYPE.itemsize, dtype=torch.uint8, device=d),
+                torch.zeros(q.n * N.HIST_BINS, dtype=torch.int32, device=d))
+
+    stream = torch.cuda.current_stream().cuda_stream
+    ref = outputs()
+    N.check(gx.lib().gx_search_device(dev.handle, ws.handle, C.byref(cq), C.byref(cp), ref[0].data_ptr(),
+                                      ref[1].data_ptr(), ref[2].data_ptr(), stream))
+    runs = []
+    for _ in range(2):
+        o = outputs()
+        N.check(gx.lib().gx_search_device_noalloc(dev.handle, C.byref(cq), C.byref(cp), o[0].data_ptr(),
+                                                  o[1].data_ptr(), o[2].data_ptr(), stream))
+        runs.append(o)
+    torch.cuda.synchronize()
+
+    rr = ref[0].cpu().numpy().view(N.RESULT_DTYPE)
+    assert (rr["status"] & 1).sum() > 0
+    for o in runs:
+        r = o[0].cpu().numpy().view(N.RESULT_DTYPE)
+        for f in ("cpsms", "status", "maxhyp", "mu", "beta", "stt1", "end1"):
+            assert np.array_equal(r[f], rr[f]), f
+        for f in ("psid", "idxoffset", "sharedions", "totalions"):
+            assert np.array_equal(r["top"][f], rr["top"][f]), f
+        assert np.array_equal(r["top"]["hyperscore"].view(np.uint32), rr["top"]["hyperscore"].view(np.uint32))
+        m = (rr["status"] & 1) != 0
+        np.testing.assert_allclose(r["e_x"][m], rr["e_x"][m], rtol=1e-9)
+        np.testing.assert_allclose(r["e_fp64"][m], rr["e_fp64"][m], rtol=1e-9)
+        assert torch.equal(o[1], ref[1]) and torch.equal(o[2], ref[2])
+
+
+def test_noalloc_rejects_batches_beyond_its_scratch(golden):
+    if not has_gpu():
+        pytest.skip("no CUDA device")
+    import gicops_b200 as gx
+    import gicops_b200._native as N
+
+    c = golden("closed_small")
+    dev = gx.DeviceIndex(c["index"], 0)
+    nspec = N.NOALLOC_MAX_WINDOWS // dev.host.nlen + 1
+    cq = N.Queries(nspec, 0, None, None, None, None, None, None)      # refused before any pointer is read
+    cp = search_params(c, flags=gx.FLAG_PLAIN).c()
+    rc = gx.lib().gx_search_device_noalloc(dev.handle, C.byref(cq), C.byref(cp), 1, None, None, None)
+    assert rc == -3004
+    assert b"exceeds the fixed scratch" in gx.lib().gx_last_error()
