@@ -6,11 +6,11 @@ of include/gicops_b200.h.  A drop-in for the reference's (mhaseeb123/gicops)
 ``hcp::gpu::cuda::s3::search`` / ``DSLIM_QuerySpectrum`` boundary.
 """
 
-from . import synth
+from . import synth, tail
 from ._native import (CELL_DTYPE, FLAG_PLAIN, FLAG_WIDE_SCORECARD, HIST_BINS, PEP_ENTRY_DTYPE, RESULT_DTYPE,
                       GxError, lib)
 from .index import DeviceIndex, HostIndex
 from .search import Searcher, SearchParams, SearchResults
 
-__all__ = ["synth", "lib", "GxError", "HostIndex", "DeviceIndex", "Searcher", "SearchParams", "SearchResults",
+__all__ = ["synth", "tail", "lib", "GxError", "HostIndex", "DeviceIndex", "Searcher", "SearchParams", "SearchResults",
            "RESULT_DTYPE", "CELL_DTYPE", "PEP_ENTRY_DTYPE", "HIST_BINS", "FLAG_PLAIN", "FLAG_WIDE_SCORECARD"]

@@ -28,6 +28,16 @@ STATUS_NAMES = {
 
 FLAG_WIDE_SCORECARD = 1
 FLAG_PLAIN = 2
+STATUS_LEARNED_TAIL = 16
+
+TAIL_WINDOW = 128
+TAIL_IN = 132
+TAIL_HIDDEN = 256
+TAIL_OUT = 2
+TAIL_NPARAM = TAIL_HIDDEN * TAIL_IN + TAIL_HIDDEN + TAIL_HIDDEN * TAIL_HIDDEN + TAIL_HIDDEN + TAIL_OUT * TAIL_HIDDEN \
+    + TAIL_OUT
+TAIL_MAX_KEEP = 512
+TAIL_SAMPLE_DTYPE = np.dtype([("query", "<u4"), ("keep", "<u4"), ("seed", "<u8")])
 
 CELL_DTYPE = np.dtype([("hyperscore", "<f4"), ("psid", "<i4"), ("idxoffset", "<u2"),
                        ("sharedions", "<u2"), ("totalions", "<u2"), ("pad", "<u2")])
@@ -82,6 +92,11 @@ class Queries(C.Structure):
                 ("intn", C.c_void_p), ("prec", C.c_void_p), ("charge", C.c_void_p), ("dM", C.c_void_p)]
 
 
+class TailAdam(C.Structure):
+    _fields_ = [("lr", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float),
+                ("w_slope", C.c_float), ("w_lgs", C.c_float)]
+
+
 _lib = None
 
 # (name, restype, argtypes) of every exported entry point
@@ -109,6 +124,24 @@ _SIGS = [
     ("gx_lgfact", None, [C.c_void_p]),
     ("gx_profile_enable", C.c_int32, [C.c_int32]),
     ("gx_profile_read", C.c_int32, [C.c_void_p, C.c_int32]),
+    ("gx_tail_model_create", C.c_int32, [C.c_int32, C.c_uint32, C.c_uint64, C.POINTER(C.c_void_p)]),
+    ("gx_tail_model_free", C.c_int32, [C.c_void_p]),
+    ("gx_tail_model_set", C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("gx_tail_model_get", C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_uint64)]),
+    ("gx_tail_features", C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                                     C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_void_p]),
+    ("gx_tail_fit_rows", C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
+    ("gx_tail_grad", C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
+                                 C.c_void_p, C.c_void_p]),
+    ("gx_tail_train_step", C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(TailAdam),
+                                       C.c_void_p, C.c_void_p]),
+    ("gx_tail_predict", C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
+    ("gx_tail_apply", C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                                  C.c_uint32, C.c_double, C.c_void_p]),
+    ("gx_tail_check", C.c_int32, [C.c_void_p]),
+    ("gx_tail_gemm", C.c_int32, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_int64, C.c_int64, C.c_int32,
+                                 C.c_int32, C.c_int32, C.c_void_p, C.c_int64, C.c_void_p]),
     ("gx_last_error", C.c_char_p, []),
     ("gx_launch_count", C.c_uint64, []),
 ]
@@ -131,6 +164,7 @@ def lib():
             f.restype = res
             f.argtypes = args
         assert C.sizeof(Params) == 48 and RESULT_DTYPE.itemsize == 80 and CELL_DTYPE.itemsize == 16
+        assert TAIL_SAMPLE_DTYPE.itemsize == 16 and C.sizeof(TailAdam) == 24
         _lib = L
     return _lib
 

@@ -151,7 +151,8 @@ typedef struct {
 
 /* Per-spectrum result.  status bits: 1 = cpsms >= min_cpsm (e-value computed),
  * 2 = e_x < expect_max (a PSM the reference prints), 4 = a shared-ion count above
- * MAX_SHDPEAKS (80) was clamped, 8 = the 12-byte scorecard was used. */
+ * MAX_SHDPEAKS (80) was clamped, 8 = the 12-byte scorecard was used, 16 = the e-value
+ * comes from the learned tail (gx_tail_apply). */
 typedef struct {
     int32_t cpsms;
     int32_t status;
@@ -219,6 +220,90 @@ typedef struct {
 } gx_kernel_time;
 gx_status gx_profile_enable(int32_t on);
 int32_t gx_profile_read(gx_kernel_time *out, int32_t cap);
+
+/* ---- learned tail (no counterpart in the reference) ---------------------------------
+ * A small MLP that predicts a query's expeRT log-survival line from its score histogram,
+ * for queries whose histogram holds too few candidates for a stable plain fit
+ * (source/core/expeRT.cpp ModelTailFit is the plain fit it stands in for).
+ *
+ * Input (GX_TAIL_IN features, bf16): log10(1 + count) of the GX_TAIL_WINDOW histogram
+ * bins from the first non-empty bin b0, then log10(candidates), precursor mass / 1000,
+ * charge, (maxhyp - b0) / 100.  Network 132 -> 256 -> 256 -> 2 with GELU (erf form);
+ * bf16 weights and activations, fp32 accumulation on the tensor cores, fp32 master
+ * weights and Adam.  Output: the line's slope (per histogram bin) and its value at
+ * maxhyp (log10 survival fraction); the intercept is value - slope * maxhyp.
+ *
+ * Parameters (fp32, GX_TAIL_NPARAM): W1 [256][132], b1 [256], W2 [256][256], b2 [256],
+ * W3 [2][256], b3 [2] (row-major, out x in).  norm[4] = mean and scale of the two
+ * targets (slope, value); the network works on normalised targets. */
+#define GX_TAIL_WINDOW 128
+#define GX_TAIL_IN     132
+#define GX_TAIL_HIDDEN 256
+#define GX_TAIL_OUT    2
+#define GX_TAIL_NPARAM (GX_TAIL_HIDDEN * GX_TAIL_IN + GX_TAIL_HIDDEN + GX_TAIL_HIDDEN * GX_TAIL_HIDDEN + \
+                        GX_TAIL_HIDDEN + GX_TAIL_OUT * GX_TAIL_HIDDEN + GX_TAIL_OUT)
+#define GX_TAIL_MAX_KEEP 512          /* largest subsample drawn by gx_tail_features */
+#define GX_STATUS_LEARNED_TAIL 16     /* gx_result.status: e_x, mu, beta come from the model */
+
+typedef struct gx_tail_model gx_tail_model;
+
+/* One feature row: histogram row `query`; keep > 0 subsamples its candidates to `keep`
+ * (the top-scoring one always kept, the others drawn without replacement by Floyd's
+ * method from a SplitMix64 stream seeded with `seed`); keep = 0 uses them all. */
+typedef struct {
+    uint32_t query;
+    uint32_t keep;
+    uint64_t seed;
+} gx_tail_sample;
+
+typedef struct {
+    float lr, beta1, beta2, eps;  /* Adam */
+    float w_slope, w_lgs;         /* loss weights of the two normalised outputs */
+} gx_tail_adam;
+
+/* Model with scratch for batches of up to max_batch rows; weights U(+-1/sqrt(fan_in))
+ * from std::mt19937_64(seed), biases 0, norm = {0, 1, 0, 1}. */
+gx_status gx_tail_model_create(int32_t device, uint32_t max_batch, uint64_t seed, gx_tail_model **out);
+gx_status gx_tail_model_free(gx_tail_model *m);
+/* Host copies in/out (either pointer may be NULL).  set resets the Adam state; it synchronises. */
+gx_status gx_tail_model_set(gx_tail_model *m, const float *params, const float *norm);
+gx_status gx_tail_model_get(const gx_tail_model *m, float *params, float *norm, uint64_t *steps);
+
+/* Feature rows for n samples (host array) of the nq queries whose histograms
+ * (hist_dev [nq][GX_HIST_BINS]), results (maxhyp), precursor masses and charges (may be
+ * NULL: 0) are on the device.  Writes x_dev [n][GX_TAIL_IN] (bf16 bits) and, when not
+ * NULL, the subsampled histograms [n][GX_HIST_BINS], their candidate counts and maxhyp.
+ * n <= max_batch.  Synchronises the stream. */
+gx_status gx_tail_features(gx_tail_model *m, const uint32_t *hist_dev, const gx_result *res_dev,
+                           const float *prec_dev, const int32_t *charge_dev, uint32_t nq,
+                           const gx_tail_sample *samples_host, uint32_t n, uint16_t *x_dev,
+                           uint32_t *sub_hist_dev, int32_t *sub_cpsms_dev, int32_t *hyp_dev, void *stream);
+/* Plain FP64 expeRT fit of n histogram rows: fit_dev [n][2] = (slope, intercept). */
+gx_status gx_tail_fit_rows(const uint32_t *hist_dev, const int32_t *cpsms_dev, const int32_t *hyp_dev, uint32_t n,
+                           double *fit_dev, void *stream);
+/* Forward + loss + backward on n rows; targets [n][2] = (slope, value at maxhyp).
+ * grad_dev (optional) receives the GX_TAIL_NPARAM gradients, loss_dev (optional) the
+ * mean loss.  weights2 (host, optional) = loss weights of the two outputs (default 1, 1). */
+gx_status gx_tail_grad(gx_tail_model *m, const uint16_t *x_dev, const float *target_dev, uint32_t n,
+                       const float *weights2, float *grad_dev, float *loss_dev, void *stream);
+/* One Adam step on a batch (gx_tail_grad followed by the update). */
+gx_status gx_tail_train_step(gx_tail_model *m, const uint16_t *x_dev, const float *target_dev, uint32_t n,
+                             const gx_tail_adam *opt, float *loss_dev, void *stream);
+/* pred_dev [n][2] = (slope, log10 survival fraction at maxhyp). */
+gx_status gx_tail_predict(gx_tail_model *m, const uint16_t *x_dev, uint32_t n, float *pred_dev, void *stream);
+/* Fallback policy over search results on the device: every query with status & 1 and
+ * cpsms < sparse_below takes the learned line when it is finite and falling
+ * (mu, beta, e_x replaced, status |= GX_STATUS_LEARNED_TAIL, bit 2 re-evaluated against
+ * expect_max); all others keep the plain fit.  slope, icpt and e_fp64 keep the plain fit. */
+gx_status gx_tail_apply(gx_tail_model *m, const uint32_t *hist_dev, gx_result *res_dev, const float *prec_dev,
+                        const int32_t *charge_dev, uint32_t nspec, uint32_t sparse_below, double expect_max,
+                        void *stream);
+/* Synchronises and reports a device-side guard of the model's kernels. */
+gx_status gx_tail_check(gx_tail_model *m);
+/* The model's tensor-core GEMM alone: D[M][N] (fp32, row stride ldd) = A * B^T with
+ * A(m,k) = a[m*sam + k*sak], B(n,k) = b[n*sbn + k*sbk] (bf16 bits), on the current device. */
+gx_status gx_tail_gemm(const uint16_t *a_dev, int64_t sam, int64_t sak, const uint16_t *b_dev, int64_t sbn,
+                       int64_t sbk, int32_t M, int32_t N, int32_t K, float *d_dev, int64_t ldd, void *stream);
 
 /* Message of the calling thread's last failure ("" if none). */
 const char *gx_last_error(void);
