@@ -166,41 +166,40 @@ __global__ void __launch_bounds__(kPrepBlock) k_prep(SearchArgs a, int2 *win, ui
 // ------------------------------------------------------------------------------------
 constexpr int kBBlock = 1024;
 constexpr int kBWarps = kBBlock / 32;
-constexpr int kPend = 64;       // per-warp queue of candidates awaiting a hyperscore
-constexpr int kIvlChunk = 1024; // intervals per span table
-constexpr int kUnit = 256;      // ids per warp work unit
-constexpr int kIlp = 8;         // iA loads in flight per lane
-constexpr int kEntSmem = 4;     // heap entrants per warp kept in shared memory
+constexpr int kPend = 96;       // per-warp queue of candidates awaiting a hyperscore (32 + one scan step)
+constexpr int kIvlChunk = 512;  // intervals per span table
+constexpr int kChunks = 4;      // 16-byte id chunks in flight per lane
+constexpr int kEntSmem = 8;     // heap entrants per warp kept in shared memory
 
-// Dynamic shared memory after the scorecard tile:
-//   queued candidates a = packed word (or wide counts | b-sum << 32),
-//                     b = candidate offset in the tile | wide y-sum << 32;
-//   span table of the current length: iA start, flat prefix and (S, c) per interval.
+// Dynamic shared memory after the scorecard tile (tile * 8 bytes):
+//   pend       per-warp queue of candidate offsets awaiting a hyperscore
+//   span table of up to kIvlChunk intervals, in the current block of the current length
+//              (element indices relative to the length's 16-byte aligned base):
+//              q0 = 16-byte chunk of the first id, [a0, a1) = the interval's ids,
+//              c, S = coverage count and intensity sum, pre = exclusive prefix of the
+//              intervals' chunk counts (kIvlChunk + 1)
 struct BatchDyn {
-    unsigned long long (*pend_a)[kPend];
-    unsigned long long (*pend_b)[kPend];
-    uint32_t *sp_start;
-    uint32_t *sp_pre;
-    uint2 *sp_cs;
+    uint32_t (*pend)[kPend];
+    uint32_t *sp_q0, *sp_a0, *sp_a1, *sp_c, *sp_S, *sp_pre;
 };
 
-__host__ __device__ constexpr size_t batch_dyn_bytes() {
-    return sizeof(unsigned long long) * kBWarps * kPend * 2 + sizeof(uint2) * kIvlChunk +
-           sizeof(uint32_t) * (2 * kIvlChunk + 4);
+__host__ __device__ constexpr size_t batch_dyn_bytes(int)
+{
+    return sizeof(uint32_t) * ((size_t)kBWarps * kPend + 5 * (size_t)kIvlChunk + (kIvlChunk + 4));
 }
 
 __device__ __forceinline__ BatchDyn carve_dyn(unsigned char *base)
 {
     BatchDyn d;
-    d.pend_a = reinterpret_cast<unsigned long long (*)[kPend]>(base);
-    base += sizeof(unsigned long long) * kBWarps * kPend;
-    d.pend_b = reinterpret_cast<unsigned long long (*)[kPend]>(base);
-    base += sizeof(unsigned long long) * kBWarps * kPend;
-    d.sp_cs = reinterpret_cast<uint2 *>(base);
-    base += sizeof(uint2) * kIvlChunk;
-    d.sp_start = reinterpret_cast<uint32_t *>(base);
-    base += sizeof(uint32_t) * kIvlChunk;
-    d.sp_pre = reinterpret_cast<uint32_t *>(base);
+    uint32_t *p = reinterpret_cast<uint32_t *>(base);
+    d.pend = reinterpret_cast<uint32_t (*)[kPend]>(p);
+    p += kBWarps * kPend;
+    d.sp_q0 = p; p += kIvlChunk;
+    d.sp_a0 = p; p += kIvlChunk;
+    d.sp_a1 = p; p += kIvlChunk;
+    d.sp_c = p; p += kIvlChunk;
+    d.sp_S = p; p += kIvlChunk;
+    d.sp_pre = p;
     return d;
 }
 
@@ -217,22 +216,25 @@ struct BatchSmem {
     int32_t status;
     int32_t spec;
     uint32_t next_unit;
+    uint32_t ent_mask;               // warps with entrants in the last scored tile
     float root;
 };
 
-// Device ids are 2*entry + (y ion); ids of the tile satisfy id - base < lim with
-// base = 2*t0, lim = 2*tn.  The scorecard keeps b ions in [0, T) and y ions in [T, 2T).
-__device__ __forceinline__ void scatter_packed(uint32_t *sc, uint32_t id, uint32_t base, uint32_t lim, uint32_t T,
-                                               uint32_t vb)
+// Block-local ids are 2*(entry - block start) + (y ion); the tile's ids satisfy
+// id - lo < lim.  Packed scorecard: per candidate a b word and a y word (count << 24 |
+// intensity sum), interleaved, so that id - lo is the word an id adds to; 32-bit adds
+// whose old values are not needed.
+__device__ __forceinline__ void scatter_packed(uint32_t *sc, uint32_t id, uint32_t lo, uint32_t lim, uint32_t vb)
 {
-    const uint32_t rel = id - base;
-    if (rel < lim) atomicAdd(sc + (rel >> 1) + (rel & 1u) * T, vb);
+    const uint32_t rel = id - lo;
+    if (rel < lim) atomicAdd(sc + rel, vb);
 }
 
-__device__ __forceinline__ void scatter_wide(uint32_t *cnt, uint32_t *ib, uint32_t *iy, uint32_t id, uint32_t base,
+// Wide scorecard (12 bytes): counts b | y << 16, intensity sums of b and y ions.
+__device__ __forceinline__ void scatter_wide(uint32_t *cnt, uint32_t *ib, uint32_t *iy, uint32_t id, uint32_t lo,
                                              uint32_t lim, uint32_t c, uint32_t S)
 {
-    const uint32_t rel = id - base;
+    const uint32_t rel = id - lo;
     if (rel < lim) {
         const uint32_t cand = rel >> 1;
         const bool y = rel & 1u;
@@ -244,22 +246,23 @@ __device__ __forceinline__ void scatter_wide(uint32_t *cnt, uint32_t *ib, uint32
 // Hyperscores of up to 32 queued candidates (one per lane), in queue order: the
 // histogram and candidate count take every PSM; PSMs with h >= tau go, in order, to
 // the warp's entrant list for the exact heap.
-__device__ __forceinline__ void score_queue(BatchSmem &sm, const BatchDyn &dd, const SearchArgs &a, int wid, int lane,
-                                            int n, int t0,
-                                            int ixx, uint32_t speclen, float tau, bool wide, Cell *ent, int &nent,
-                                            int &cps)
+__device__ __forceinline__ void score_queue(BatchSmem &sm, const BatchDyn &dd, const void *scv, int ctile, int wid,
+                                            int lane, int n, int t0, int ixx, uint32_t speclen, float tau, bool wide,
+                                            Cell *ent, int &nent, int &cps)
 {
     bool psm = false;
     Cell cell;
     if (lane < n) {
-        const unsigned long long va = dd.pend_a[wid][lane], vb = dd.pend_b[wid][lane];
+        const uint32_t off = dd.pend[wid][lane];
         uint32_t bc, yc, ib, iy;
         if (!wide) {
-            const uint32_t lo = (uint32_t)va, hi = (uint32_t)(va >> 32);
-            bc = lo >> 24; ib = lo & 0xFFFFFFu; yc = hi >> 24; iy = hi & 0xFFFFFFu;
+            const uint2 v = reinterpret_cast<const uint2 *>(scv)[off];
+            bc = v.x >> 24; ib = v.x & 0xFFFFFFu; yc = v.y >> 24; iy = v.y & 0xFFFFFFu;
         } else {
-            bc = (uint32_t)va & 0xFFFFu; yc = (uint32_t)va >> 16;
-            ib = (uint32_t)(va >> 32); iy = (uint32_t)(vb >> 32);
+            const uint32_t *cnt = reinterpret_cast<const uint32_t *>(scv);
+            const uint32_t cv = cnt[off];
+            bc = cv & 0xFFFFu; yc = cv >> 16;
+            ib = cnt[ctile + off]; iy = cnt[2 * ctile + off];
         }
         uint32_t bi = bc, yi = yc;
         if (bi > 80u || yi > 80u) {
@@ -268,16 +271,14 @@ __device__ __forceinline__ void score_queue(BatchSmem &sm, const BatchDyn &dd, c
             yi = min(yi, 80u);
         }
         const double h1 = sm.lgf[bi] + sm.lgf[yi];
-        const uint32_t xb = 1u + ib, xy = 1u + iy;
-        // log10 of small integers from a table filled by the same log10 (identical values)
-        const double lb = xb < a.logtab_n ? __ldg(a.logtab + xb) : log10((double)xb);
-        const double ly = xy < a.logtab_n ? __ldg(a.logtab + xy) : log10((double)xy);
+        // every lane evaluates both logarithms: no divergence, no table traffic
+        const double lb = log10((double)(1u + ib)), ly = log10((double)(1u + iy));
         float h = __double2float_rn(h1 + lb + ly - 4.0);
         if (h > 0.0f) {
             if (h >= 80.0f) h = 79.0f;
             psm = true;
             cell.h = h;
-            cell.psid = t0 + (int)(uint32_t)vb;
+            cell.psid = t0 + (int)off;
             cell.ixx = (uint16_t)ixx;
             cell.shp = (uint16_t)((bc + yc) & 0xFFFFu);
             cell.total = (uint16_t)speclen;
@@ -307,9 +308,9 @@ __device__ __noinline__ void heap_insert_many(Cell *heap, int *size, int cap, co
     *size = hs;
 }
 
-// Bring iA span [st, en) of a block into L2 ahead of its tile: one bulk prefetch per span,
-// rounded out to 16-byte boundaries inside the iAb allocation.
-__device__ __forceinline__ void prefetch_span(const uint32_t *iAb_base, uint64_t iab_bytes, const uint32_t *iA,
+// Bring the ids [st, en) (element indices) of a block into L2 ahead of its tile: one bulk
+// prefetch per span, rounded out to 16-byte boundaries inside the iAb allocation.
+__device__ __forceinline__ void prefetch_span(const uint16_t *iAb_base, uint64_t iab_bytes, const uint16_t *iA,
                                               uint32_t st, uint32_t en)
 {
     if (en <= st) return;
@@ -322,12 +323,14 @@ __device__ __forceinline__ void prefetch_span(const uint32_t *iAb_base, uint64_t
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(lo), "r"((uint32_t)(hi - lo)) : "memory");
 }
 
-// Thread 0 inserts the entrants of warps 0..31 of the last scanned tile, in order: the
-// first few of each warp from shared memory, any overflow from the warp's global spill.
+// Thread 0 inserts the entrants of the warps that have some (in warp order) of the last
+// scored tile: the first few of each warp from shared memory, any overflow from the
+// warp's global spill.
 __device__ __noinline__ void insert_entrants(BatchSmem &sm, const Cell *spill_cta, uint32_t spill_per_warp, int cap)
 {
     int hs = sm.heap_size;
-    for (int w2 = 0; w2 < kBWarps; w2++) {
+    for (uint32_t mask = sm.ent_mask; mask; mask &= mask - 1u) {
+        const int w2 = __ffs(mask) - 1;
         const int n2 = sm.warp_cnt[w2];
         const int ns = min(n2, kEntSmem);
         for (int k = 0; k < ns; k++) heap_insert(sm.heap, hs, cap, sm.ent_s[w2][k]);
@@ -346,22 +349,32 @@ __device__ __noinline__ void insert_entrants(BatchSmem &sm, const Cell *spill_ct
     }
     sm.heap_size = hs;
     sm.root = sm.heap[0].h;
+    sm.ent_mask = 0u;
 }
 
-// Span table of up to kIvlChunk intervals for one length: iA start of each interval's
-// bins, exclusive prefix of their id counts (the flat id space), coverage (S, c).
+// Span table of up to kIvlChunk intervals for one block of one length (element indices
+// relative to the length's aligned base, which lies rel0 elements before its first id),
+// and the exclusive prefix of the intervals' 16-byte chunk counts.  With `have`, thread i
+// already holds the block offsets of interval i (loaded one tile ahead).
 __device__ __forceinline__ void build_span_table(BatchSmem &sm, const BatchDyn &dd, const Interval *iv, uint32_t n,
-                                                 const uint32_t *__restrict__ bA, int tid, int lane, int wid)
+                                                 const uint32_t *__restrict__ bA, uint32_t rel0, bool have,
+                                                 uint32_t have_s, uint32_t have_e, int tid, int lane, int wid)
 {
     uint32_t cnt = 0;
     if (tid < (int)n) {
         const Interval v = iv[tid];
-        const uint32_t b = __ldg(bA + v.b0), e = __ldg(bA + v.b1 + 1);
-        dd.sp_start[tid] = b;
-        dd.sp_cs[tid] = make_uint2(v.S, v.c);
-        cnt = e - b;
+        const uint32_t a0 = rel0 + (have ? have_s : __ldg(bA + v.b0));
+        const uint32_t a1 = rel0 + (have ? have_e : __ldg(bA + v.b1 + 1));
+        const uint32_t q0 = a0 >> 3;
+        cnt = a1 > a0 ? ((a1 + 7u) >> 3) - q0 : 0u;
+        dd.sp_q0[tid] = q0;
+        dd.sp_a0[tid] = a0;
+        dd.sp_a1[tid] = a1;
+        dd.sp_c[tid] = v.c;
+        dd.sp_S[tid] = v.S;
     }
-    // block exclusive scan of cnt (kBBlock == kIvlChunk)
+    if (tid == 0) sm.next_unit = 0;
+    // block exclusive scan of cnt
     uint32_t x = cnt;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -386,6 +399,76 @@ __device__ __forceinline__ void build_span_table(BatchSmem &sm, const BatchDyn &
     if (n == 0 && tid == 0) dd.sp_pre[0] = 0;
 }
 
+// Stream the ids of every interval of the span table into the scorecard.  Warps take
+// units of 32 x kChunks consecutive 16-byte chunks (8 ids each) from a shared counter;
+// lane l loads chunks l, l+32, ... of the unit, all before it scatters any.
+__device__ __forceinline__ void stream_tile(BatchSmem &sm, const BatchDyn &dd, const uint4 *__restrict__ ia4,
+                                            uint32_t ncv, void *scv, int ctile, bool wide, uint32_t lo, uint32_t lim,
+                                            int lane)
+{
+    const uint32_t M = dd.sp_pre[ncv];
+    uint32_t *cnt = reinterpret_cast<uint32_t *>(scv);
+    for (;;) {
+        uint32_t u = 0;
+        if (lane == 0) u = atomicAdd(&sm.next_unit, 1u);
+        u = __shfl_sync(0xffffffffu, u, 0);
+        const uint32_t j0 = u * (32u * kChunks);
+        if (j0 >= M) break;
+        // interval of the unit's first chunk; each lane walks on from there
+        uint32_t k = 0, hi = ncv;
+        while (hi - k > 1) {
+            const uint32_t mid = (k + hi) >> 1;
+            if (dd.sp_pre[mid] <= j0) k = mid; else hi = mid;
+        }
+        uint4 v[kChunks];
+        uint32_t kx[kChunks];
+#pragma unroll
+        for (int p = 0; p < kChunks; p++) {
+            const uint32_t j = j0 + (uint32_t)lane + 32u * p;
+            kx[p] = 0xFFFFFFFFu;
+            if (j < M) {
+                while (dd.sp_pre[k + 1] <= j) k++;
+                kx[p] = k;
+                v[p] = __ldg(ia4 + (dd.sp_q0[k] + (j - dd.sp_pre[k])));
+            }
+        }
+#pragma unroll
+        for (int p = 0; p < kChunks; p++) {
+            if (kx[p] == 0xFFFFFFFFu) continue;
+            const uint32_t kk = kx[p];
+            const uint32_t j = j0 + (uint32_t)lane + 32u * p;
+            const uint32_t eq = (dd.sp_q0[kk] + (j - dd.sp_pre[kk])) << 3;
+            const uint32_t a0 = dd.sp_a0[kk], a1 = dd.sp_a1[kk];
+            const uint32_t c = dd.sp_c[kk], S = dd.sp_S[kk];
+            const uint32_t w4[4] = {v[p].x, v[p].y, v[p].z, v[p].w};
+            const bool full = eq >= a0 && eq + 8u <= a1;
+            if (!wide) {
+                const uint32_t vb = (c << 24) | S;
+                if (full) {
+#pragma unroll
+                    for (int m = 0; m < 8; m++)
+                        scatter_packed(cnt, (w4[m >> 1] >> (16 * (m & 1))) & 0xFFFFu, lo, lim, vb);
+                } else {
+#pragma unroll
+                    for (int m = 0; m < 8; m++) {
+                        const uint32_t e = eq + (uint32_t)m;
+                        if (e >= a0 && e < a1)
+                            scatter_packed(cnt, (w4[m >> 1] >> (16 * (m & 1))) & 0xFFFFu, lo, lim, vb);
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int m = 0; m < 8; m++) {
+                    const uint32_t e = eq + (uint32_t)m;
+                    if (full || (e >= a0 && e < a1))
+                        scatter_wide(cnt, cnt + ctile, cnt + 2 * ctile, (w4[m >> 1] >> (16 * (m & 1))) & 0xFFFFu, lo,
+                                     lim, c, S);
+                }
+            }
+        }
+    }
+}
+
 __global__ void __launch_bounds__(kBBlock, 1) k_search_batched(SearchArgs a)
 {
     extern __shared__ __align__(16) unsigned char dyn[];
@@ -393,11 +476,12 @@ __global__ void __launch_bounds__(kBBlock, 1) k_search_batched(SearchArgs a)
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     for (int i = tid; i < 81; i += kBBlock) sm.lgf[i] = a.lgfact[i];
     const int T = a.tile;
-    uint32_t *scp = reinterpret_cast<uint32_t *>(dyn);   // packed: b words [0, T), y words [T, 2T)
+    void *scv = dyn;   // packed: T interleaved (b, y) word pairs; wide: 3 arrays of ctile words
     const BatchDyn dd = carve_dyn(dyn + (size_t)T * 8);
     for (int i = tid; i < 2 * T; i += kBBlock) reinterpret_cast<uint32_t *>(dyn)[i] = 0;
     // this warp's entrant list (global scratch, one slot per candidate of its range)
     Cell *ent = a.spill + ((uint64_t)blockIdx.x * kBWarps + wid) * (uint64_t)a.spill_per_warp;
+    const uint32_t minshp = a.min_shp;
 
     for (;;) {
         __syncthreads();
@@ -408,6 +492,7 @@ __global__ void __launch_bounds__(kBBlock, 1) k_search_batched(SearchArgs a)
             sm.cpsms = 0;
             sm.status = 0;
             sm.root = 0.0f;
+            sm.ent_mask = 0u;
         }
         for (int i = tid; i < kHist; i += kBBlock) sm.hist[i] = 0;
         __syncthreads();
@@ -426,20 +511,26 @@ __global__ void __launch_bounds__(kBBlock, 1) k_search_batched(SearchArgs a)
         }
         const bool wide = a.guard[s] == 0 || (a.flags & GX_FLAG_WIDE_SCORECARD);
         if (tid == 0 && wide) sm.status |= 8;
-        const int ctile = wide ? (T * 2) / 3 : T;
-        uint32_t *scw_cnt = reinterpret_cast<uint32_t *>(dyn);
-        uint32_t *scw_ib = scw_cnt + ctile;
-        uint32_t *scw_iy = scw_ib + ctile;
+        const int ctile = wide ? ((T * 2) / 3) & ~31 : T;
         const uint32_t nv = a.nivl[s];
         const Interval *ivl = a.ivl + 2ull * a.qidx[s];
         int cps = 0;   // candidate PSMs counted by this warp (lane 0 adds them at the end)
         bool heap_due = false;
+        // Offsets of the next tile's bins, loaded by thread i for interval i one tile ahead
+        // (when all intervals fit one span table): they feed the L2 prefetch of that tile's
+        // ids and its span table.
+        uint32_t nx_s = 0, nx_e = 0;
+        int nx_len = -1;
+        int64_t nx_kb = -1;
+        const bool carry = nv <= (uint32_t)kIvlChunk;
 
         for (int ixx = 0; ixx < a.nlen; ixx++) {
             const int2 w = a.win[(uint64_t)s * a.nlen + ixx];
             if (w.y < w.x) continue;
             const DevLen ln = a.lens[ixx];
-            const uint32_t *__restrict__ iA = a.iAb + ln.ia_off;   // block layout
+            const uint64_t base = ln.ia_off & ~7ull;              // 16-byte aligned
+            const uint32_t rel0 = (uint32_t)(ln.ia_off - base);
+            const uint4 *__restrict__ ia4 = reinterpret_cast<const uint4 *>(a.iAb + base);
             const uint32_t speclen = ln.speclen;
             const int64_t E = a.block;
             const int64_t kb0 = w.x / E, kb1 = w.y / E;
@@ -448,207 +539,132 @@ __global__ void __launch_bounds__(kBBlock, 1) k_search_batched(SearchArgs a)
               const uint32_t *__restrict__ bA = a.blkA + ln.blk_off + (uint64_t)kb * (a.nbins + 1);
               const int bt0 = (int)max((int64_t)w.x, kb * E), bt1 = (int)min((int64_t)w.y + 1, (kb + 1) * E);
               const int nsub = (bt1 - bt0 + ctile - 1) / ctile;
+              const bool have = carry && nx_len == ixx && nx_kb == kb;   // offsets loaded a tile ago
+              const uint32_t cur_s = nx_s, cur_e = nx_e;
+              // the next tile of this spectrum: the next block of this length, or the first
+              // block of the next length with a window
+              int nx = -1;
+              int64_t nkb = 0;
+              if (kb < kb1) {
+                  nx = ixx;
+                  nkb = kb + 1;
+              } else {
+                  for (int j = ixx + 1; j < a.nlen; j++) {
+                      const int2 w2 = a.win[(uint64_t)s * a.nlen + j];
+                      if (w2.y >= w2.x) {
+                          nx = j;
+                          nkb = w2.x / E;
+                          break;
+                      }
+                  }
+              }
+              const uint16_t *niA = nullptr;
+              if (carry && nx >= 0) {
+                  const DevLen nl = a.lens[nx];
+                  niA = a.iAb + nl.ia_off;
+                  if (tid < (int)nv) {
+                      const uint32_t *nbA = a.blkA + nl.blk_off + (uint64_t)nkb * (a.nbins + 1);
+                      const Interval v = ivl[tid];
+                      nx_s = __ldg(nbA + v.b0);      // in flight while this tile streams
+                      nx_e = __ldg(nbA + v.b1 + 1);
+                  }
+              }
+              nx_len = nx;
+              nx_kb = nkb;
               for (int ti = 0; ti < nsub; ti++) {
                 const int t0 = bt0 + ti * ctile;
                 const int t1 = min(bt1, t0 + ctile);
                 const int tn = t1 - t0;
                 if (tn <= 0) continue;
-                const uint32_t idlo = 2u * (uint32_t)t0, span = 2u * (uint32_t)tn;
-                // ---- stream every interval's iA span into the scorecard -----------------
+                const uint32_t lo = 2u * (uint32_t)(t0 - kb * E), lim = 2u * (uint32_t)tn;
+                // ---- stream every interval's ids into the scorecard ----------------------
                 for (uint32_t ic0 = 0; ic0 < nv; ic0 += kIvlChunk) {
                     const uint32_t ncv = min((uint32_t)kIvlChunk, nv - ic0);
                     if (ti == 0 || nv > (uint32_t)kIvlChunk)
-                        build_span_table(sm, dd, ivl + ic0, ncv, bA, tid, lane, wid);
-                    if (tid == 0) sm.next_unit = 0;
+                        build_span_table(sm, dd, ivl + ic0, ncv, bA, rel0, have, cur_s, cur_e, tid, lane, wid);
+                    else if (tid == 0)
+                        sm.next_unit = 0;
                     __syncthreads();
                     if (heap_due) {          // the previous tile's entrants, off the critical path
                         if (tid == 0) insert_entrants(sm, a.spill + (uint64_t)blockIdx.x * kBWarps * a.spill_per_warp, a.spill_per_warp, a.heap_cap);
                         heap_due = false;
                     }
-                    if (ic0 == 0 && ti + 1 == nsub) {
-                        // the next tile of this spectrum: the next block of this length, or the
-                        // first block of the next length with a window; prefetch its spans into L2
-                        int nx = -1;
-                        int64_t nkb = 0;
-                        if (kb < kb1) {
-                            nx = ixx;
-                            nkb = kb + 1;
-                        } else {
-                            for (int j = ixx + 1; j < a.nlen; j++) {
-                                const int2 w2 = a.win[(uint64_t)s * a.nlen + j];
-                                if (w2.y >= w2.x) {
-                                    nx = j;
-                                    nkb = w2.x / E;
-                                    break;
-                                }
-                            }
-                        }
-                        if (nx >= 0) {
-                            const DevLen nl = a.lens[nx];
-                            const uint32_t *nbA = a.blkA + nl.blk_off + (uint64_t)nkb * (a.nbins + 1);
-                            const uint32_t *niA = a.iAb + nl.ia_off;
-                            for (uint32_t i = tid; i < nv; i += kBBlock) {
-                                const Interval v = ivl[i];
-                                prefetch_span(a.iAb, a.iab_bytes, niA, __ldg(nbA + v.b0), __ldg(nbA + v.b1 + 1));
-                            }
-                        }
-                    }
-                    const uint32_t M = dd.sp_pre[ncv];
-                    for (;;) {
-                        uint32_t u = 0;
-                        if (lane == 0) u = atomicAdd(&sm.next_unit, 1u);
-                        u = __shfl_sync(0xffffffffu, u, 0);
-                        const uint32_t f0 = u * (uint32_t)kUnit;
-                        if (f0 >= M) break;
-                        const uint32_t f1 = min(M, f0 + (uint32_t)kUnit);
-                        // interval of the unit's first id (same for all lanes)
-                        uint32_t lo = 0, hi = ncv;
-                        while (hi - lo > 1) {
-                            const uint32_t mid = (lo + hi) >> 1;
-                            if (dd.sp_pre[mid] <= f0) lo = mid; else hi = mid;
-                        }
-                        // walk the unit in windows of 8 x 32 flat positions; a window spans at most
-                        // two consecutive intervals (it stops where a third one would begin)
-                        uint32_t k = lo, f = f0;
-                        while (f < f1) {
-                            while (dd.sp_pre[k + 1] <= f) k++;
-                            const uint32_t p1 = dd.sp_pre[k + 1];                 // start of interval k+1
-                            const uint32_t p2 = k + 2 <= ncv ? dd.sp_pre[min(k + 2, ncv)] : p1;
-                            const uint32_t lim = min(min(f1, f + 32u * kIlp), max(p1, p2));
-                            const uint32_t d0 = dd.sp_start[k] - dd.sp_pre[k];
-                            const uint2 c0 = dd.sp_cs[k];
-                            const bool two = k + 1 < ncv;
-                            const uint32_t d1 = two ? dd.sp_start[k + 1] - p1 : d0;
-                            const uint2 c1 = two ? dd.sp_cs[k + 1] : c0;
-                            if (!wide) {
-                                const uint32_t v0 = (c0.y << 24) | c0.x, v1 = (c1.y << 24) | c1.x;
-                                uint32_t idv[kIlp], vv[kIlp];
-#pragma unroll
-                                for (int j = 0; j < kIlp; j++) {
-                                    const uint32_t g = f + lane + 32u * j;
-                                    const bool in1 = g >= p1;
-                                    vv[j] = in1 ? v1 : v0;
-                                    idv[j] = g < lim ? __ldg(iA + (g + (in1 ? d1 : d0))) : idlo - 1u;
-                                }
-#pragma unroll
-                                for (int j = 0; j < kIlp; j++)
-                                    scatter_packed(scp, idv[j], idlo, span, (uint32_t)T, vv[j]);
-                            } else {
-                                for (uint32_t g = f + lane; g < lim; g += 32) {
-                                    const bool in1 = g >= p1;
-                                    const uint2 c = in1 ? c1 : c0;
-                                    scatter_wide(scw_cnt, scw_ib, scw_iy, __ldg(iA + (g + (in1 ? d1 : d0))), idlo, span,
-                                                 c.y, c.x);
-                                }
-                            }
-                            f = lim;
-                        }
-                    }
+                    stream_tile(sm, dd, ia4, ncv, scv, ctile, wide, lo, lim, lane);
+                    if (ti == 0 && niA && tid < (int)nv)   // the next tile's ids into L2
+                        prefetch_span(a.iAb, a.iab_bytes, niA, nx_s, nx_e);
                     __syncthreads();
                 }
-                // ---- scan: each warp owns a contiguous range, in entry order ------------
+                // ---- scan: warp w owns candidates [w*R, (w+1)*R) and takes them in entry ----
+                // order, two per lane per step (the queue never overflows: 32 + 64 slots),
+                // then clears its range for the next tile
                 const float tau = sm.heap_size < a.heap_cap ? -1.0f : sm.root;
-                const int R = (((tn + kBWarps - 1) / kBWarps) + 3) & ~3;   // multiple of 4
+                const int step = wide ? 32 : 64;
+                const int R = ((tn + kBWarps - 1) / kBWarps + step - 1) / step * step;
                 const int r0 = min(tn, wid * R), r1 = min(tn, r0 + R);
                 int npend = 0, nent = 0;
-                if (!wide) {
-                    // four candidates per lane (128-bit shared loads and stores), appended to the
-                    // queue in candidate order through a warp scan of per-lane counts
-                    for (int base = r0; base < r1; base += 128) {
-                        const int c4 = base + 4 * lane;
-                        uint4 wb = make_uint4(0, 0, 0, 0), wy = make_uint4(0, 0, 0, 0);
-                        if (c4 < r1) {
-                            wb = *reinterpret_cast<const uint4 *>(scp + c4);
-                            wy = *reinterpret_cast<const uint4 *>(scp + T + c4);
+                uint32_t *sw = reinterpret_cast<uint32_t *>(scv);
+                for (int c0 = r0; c0 < r1; c0 += step) {
+                    unsigned m = 0;
+                    if (!wide) {
+                        // lane l: candidates c, c + 1 (c = c0 + 2l), words b, y, b, y
+                        const int c = c0 + 2 * lane;
+                        if (c < r1) {
+                            const uint4 q = *reinterpret_cast<const uint4 *>(sw + 2 * c);
+                            m = ((((q.x >> 24) + (q.y >> 24)) & 0xFFFFu) >= minshp ? 1u : 0u) |
+                                ((((q.z >> 24) + (q.w >> 24)) & 0xFFFFu) >= minshp && c + 1 < r1 ? 2u : 0u);
                         }
-                        const uint32_t minshp = a.min_shp;
-                        const unsigned m = ((((wb.x >> 24) + (wy.x >> 24)) & 0xFFFFu) >= minshp ? 1u : 0u) |
-                                           ((((wb.y >> 24) + (wy.y >> 24)) & 0xFFFFu) >= minshp ? 2u : 0u) |
-                                           ((((wb.z >> 24) + (wy.z >> 24)) & 0xFFFFu) >= minshp ? 4u : 0u) |
-                                           ((((wb.w >> 24) + (wy.w >> 24)) & 0xFFFFu) >= minshp ? 8u : 0u);
-                        // order of queued entries: lane-major, bit order inside a lane
-                        const unsigned lt = (1u << lane) - 1u;
-                        const unsigned b0 = __ballot_sync(0xffffffffu, m & 1u), b1 = __ballot_sync(0xffffffffu, m & 2u);
-                        const unsigned b2 = __ballot_sync(0xffffffffu, m & 4u), b3 = __ballot_sync(0xffffffffu, m & 8u);
-                        const int total = __popc(b0) + __popc(b1) + __popc(b2) + __popc(b3);
-                        if (c4 < r1 && (wb.x | wb.y | wb.z | wb.w | wy.x | wy.y | wy.z | wy.w)) {
-                            *reinterpret_cast<uint4 *>(scp + c4) = make_uint4(0, 0, 0, 0);
-                            *reinterpret_cast<uint4 *>(scp + T + c4) = make_uint4(0, 0, 0, 0);
-                        }
-                        if (total == 0) continue;
-                        const int excl = __popc(b0 & lt) + __popc(b1 & lt) + __popc(b2 & lt) + __popc(b3 & lt);
-                        int done = 0;
-                        while (done < total) {
-                            const int room = kPend - npend;
-                            int r = 0;
-                            for (unsigned mm = m; mm; mm &= mm - 1u) {
-                                const int j = __ffs(mm) - 1;
-                                const int g = excl + r;
-                                if (g >= done && g < done + room) {
-                                    const uint32_t bj = j == 0 ? wb.x : j == 1 ? wb.y : j == 2 ? wb.z : wb.w;
-                                    const uint32_t yj = j == 0 ? wy.x : j == 1 ? wy.y : j == 2 ? wy.z : wy.w;
-                                    const int slot = npend + (g - done);
-                                    dd.pend_a[wid][slot] = (unsigned long long)bj | ((unsigned long long)yj << 32);
-                                    dd.pend_b[wid][slot] = (unsigned long long)(uint32_t)(c4 + j);
-                                }
-                                r++;
-                            }
-                            const int put = min(room, total - done);
-                            npend += put;
-                            done += put;
-                            __syncwarp();
-                            while (npend >= 32) {
-                                score_queue(sm, dd, a, wid, lane, 32, t0, ixx, speclen, tau, wide, ent, nent, cps);
-                                __syncwarp();
-                                const unsigned long long ka = lane + 32 < npend ? dd.pend_a[wid][32 + lane] : 0ull;
-                                const unsigned long long kb = lane + 32 < npend ? dd.pend_b[wid][32 + lane] : 0ull;
-                                __syncwarp();
-                                if (lane + 32 < npend) {
-                                    dd.pend_a[wid][lane] = ka;
-                                    dd.pend_b[wid][lane] = kb;
-                                }
-                                npend -= 32;
-                                __syncwarp();
-                            }
+                    } else {
+                        const int c = c0 + lane;
+                        if (c < r1) {
+                            const uint32_t cv = sw[c];
+                            m = (((cv & 0xFFFFu) + (cv >> 16)) & 0xFFFFu) >= minshp ? 1u : 0u;
                         }
                     }
-                } else {
-                    for (int base = r0; base < r1; base += 32) {
-                        const int c = base + lane;
-                        bool is = false;
-                        unsigned long long va = 0ull, vb = 0ull;
-                        if (c < r1) {
-                            const uint32_t cnt = scw_cnt[c];
-                            const uint32_t bc = cnt & 0xFFFFu, yc = cnt >> 16;
-                            va = (unsigned long long)cnt | ((unsigned long long)scw_ib[c] << 32);
-                            vb = (unsigned long long)(uint32_t)c | ((unsigned long long)scw_iy[c] << 32);
-                            scw_cnt[c] = 0; scw_ib[c] = 0; scw_iy[c] = 0;
-                            is = ((bc + yc) & 0xFFFFu) >= a.min_shp;
-                        }
-                        const unsigned bal = __ballot_sync(0xffffffffu, is);
-                        if (is) {
-                            const int slot = npend + __popc(bal & ((1u << lane) - 1u));
-                            dd.pend_a[wid][slot] = va;
-                            dd.pend_b[wid][slot] = vb;
-                        }
-                        npend += __popc(bal);
+                    // queue positions: lane order, then pair order
+                    const unsigned lt = (1u << lane) - 1u;
+                    const unsigned B0 = __ballot_sync(0xffffffffu, m & 1u), B1 = __ballot_sync(0xffffffffu, m & 2u);
+                    const int total = __popc(B0) + __popc(B1);
+                    if (total == 0) continue;
+                    int pos = npend + __popc(B0 & lt) + __popc(B1 & lt);
+                    const int cb = wide ? c0 + lane : c0 + 2 * lane;
+                    if (m & 1u) dd.pend[wid][pos++] = (uint32_t)cb;
+                    if (m & 2u) dd.pend[wid][pos] = (uint32_t)(cb + 1);
+                    npend += total;
+                    __syncwarp();
+                    while (npend >= 32) {
+                        score_queue(sm, dd, scv, ctile, wid, lane, 32, t0, ixx, speclen, tau, wide, ent, nent, cps);
                         __syncwarp();
-                        if (npend >= 32) {
-                            score_queue(sm, dd, a, wid, lane, 32, t0, ixx, speclen, tau, wide, ent, nent, cps);
-                            __syncwarp();
-                            if (lane < npend - 32) {
-                                dd.pend_a[wid][lane] = dd.pend_a[wid][32 + lane];
-                                dd.pend_b[wid][lane] = dd.pend_b[wid][32 + lane];
-                            }
-                            npend -= 32;
-                            __syncwarp();
+                        const uint32_t k0 = lane + 32 < npend ? dd.pend[wid][32 + lane] : 0u;
+                        const uint32_t k1 = lane + 64 < npend ? dd.pend[wid][64 + lane] : 0u;
+                        __syncwarp();
+                        if (lane + 32 < npend) dd.pend[wid][lane] = k0;
+                        if (lane + 64 < npend) dd.pend[wid][32 + lane] = k1;
+                        npend -= 32;
+                        __syncwarp();
+                    }
+                }
+                if (npend > 0)
+                    score_queue(sm, dd, scv, ctile, wid, lane, npend, t0, ixx, speclen, tau, wide, ent, nent, cps);
+                if (lane == 0) {
+                    sm.warp_cnt[wid] = nent;
+                    if (nent) atomicOr(&sm.ent_mask, 1u << wid);
+                }
+                // clear the warp's range [r0, r1) of every array (rounded up to 4 words: the
+                // next range starts at a multiple of 32, the arrays end at one)
+                __syncwarp();
+                if (r0 < r1) {
+                    if (!wide) {   // words [2 r0, 2 r1), two candidates per 16 bytes
+                        uint4 *z = reinterpret_cast<uint4 *>(sw);
+                        for (int i = r0 / 2 + lane; i < (r1 + 1) / 2; i += 32) z[i] = make_uint4(0u, 0u, 0u, 0u);
+                    } else {
+                        const int q0 = r0 >> 2, q1 = min(ctile, (r1 + 3) & ~3) >> 2;
+                        for (int k = 0; k < 3; k++) {
+                            uint4 *z = reinterpret_cast<uint4 *>(sw + k * ctile);
+                            for (int i = q0 + lane; i < q1; i += 32) z[i] = make_uint4(0u, 0u, 0u, 0u);
                         }
                     }
                 }
-                if (npend > 0) score_queue(sm, dd, a, wid, lane, npend, t0, ixx, speclen, tau, wide, ent, nent, cps);
-                if (lane == 0) sm.warp_cnt[wid] = nent;
                 __syncthreads();
-                // ---- exact heap: entrants of all warps, in entry order ------------------
                 heap_due = true;   // inserted by thread 0 while the next tile streams
               }
             }
@@ -684,6 +700,7 @@ __global__ void __launch_bounds__(kBBlock, 1) k_search_batched(SearchArgs a)
         }
     }
 }
+
 
 // ------------------------------------------------------------------------------------
 // k_tailfit: one warp per spectrum (the FP64 fit itself is serial in lane 0)
@@ -733,7 +750,7 @@ cudaError_t fill_logtab(double *tab, uint32_t n, cudaStream_t st)
     return cudaGetLastError();
 }
 
-size_t batched_dyn_smem(int tile) { return (size_t)tile * 8 + batch_dyn_bytes(); }
+size_t batched_dyn_smem(int tile) { return (size_t)tile * 8 + batch_dyn_bytes(tile); }
 
 cudaError_t batched_set_attributes(int tile)
 {

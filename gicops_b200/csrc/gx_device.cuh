@@ -54,10 +54,11 @@ struct SearchArgs {
     // index
     const uint32_t *bA;   // [nlen * nbins]
     const uint32_t *iA;   // bin-major CSR ids (device form 2*entry + y)
-    const uint32_t *iAb;  // block layout: per block of `block` entries, a CSR over bins
+    const uint16_t *iAb;  // block layout: per block of `block` entries, a CSR over bins of
+                          // block-local ids 2*(entry - block start) + (y ion)
     const uint32_t *blkA; // block layout offsets [nblk][nbins + 1] per length (relative to ia_off)
     uint32_t block;       // entries per block
-    uint64_t iab_bytes;   // size of iAb (bounds the L2 prefetches)
+    uint64_t iab_bytes;   // bytes of ids in iAb (bounds the L2 prefetches)
     const float *mass;
     const DevLen *lens;
     int32_t nlen;

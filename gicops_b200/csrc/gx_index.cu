@@ -7,9 +7,11 @@
 //        its ion series, which is all the query path reads from an id.  Order inside
 //        a bucket is unchanged (the plain path probes it with binary searches).
 //   iAb  the same ids regrouped by blocks of `block` consecutive entries: inside each
-//        block a CSR over the same bins (offsets blkA[block][bin], bins 0..nbins).  A
-//        candidate tile of the batched path is one block, so every bin range of a
-//        probed interval is one contiguous run of exactly the tile's ids.
+//        block a CSR over the same bins (offsets blkA[block][bin], bins 0..nbins), each
+//        id stored as 16 bits relative to its block, 2*(entry - block start) + (y ion).
+//        A candidate tile of the batched path is one block, so every bin range of a
+//        probed interval is one contiguous run of exactly the tile's ids, read as
+//        16-byte chunks of 8 ids (the allocation is padded by one chunk).
 
 #include <cub/cub.cuh>
 #include <cuda_runtime.h>
@@ -67,7 +69,7 @@ __global__ void k_blk_count(const uint32_t *iA, const uint32_t *bA, uint32_t nbi
 }
 
 __global__ void k_blk_scatter(const uint32_t *iA, const uint32_t *bA, const uint32_t *offs, uint32_t nbins, uint32_t E,
-                              uint32_t nblk, uint32_t *iAb)
+                              uint32_t nblk, uint16_t *iAb)
 {
     const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b + 1 >= nbins) return;
@@ -78,7 +80,8 @@ __global__ void k_blk_scatter(const uint32_t *iA, const uint32_t *bA, const uint
         const uint64_t key64 = 2ull * (uint64_t)(k + 1) * E;
         const uint32_t p = key64 >= 0xFFFFFFFFull ? e : lb(iA, prev, e, (uint32_t)key64);
         uint32_t d = offs[k * row + b];
-        for (uint32_t i = prev; i < p; i++) iAb[d++] = iA[i];
+        const uint32_t lo = 2u * k * E;
+        for (uint32_t i = prev; i < p; i++) iAb[d++] = (uint16_t)(iA[i] - lo);
         prev = p;
     }
 }
@@ -121,8 +124,8 @@ extern "C" gx_status gx_index_upload(const gx_length_desc *lens, int32_t nlen, u
         const uint32_t z = d.speclen / (2 * (d.peplen - 1));
         if (maxz && z != maxz) return fail(GX_ERR_INVLD_INDEX, "gx_index_upload: lengths disagree on maxz");
         maxz = z;
-        if ((uint64_t)d.npep * d.speclen >= (1ull << 32) || d.npep >= (1u << 31))
-            return fail(GX_ERR_INVLD_SIZE, "gx_index_upload: more than 2^32 ion ids in one length");
+        if ((uint64_t)d.npep * d.speclen >= (1ull << 32) - 16 || d.npep >= (1u << 31))
+            return fail(GX_ERR_INVLD_SIZE, "gx_index_upload: 2^32 - 16 or more ion ids in one length");
         if (d.npep && (!d.mass || !d.bA || !d.iA)) return fail(GX_ERR_INVLD_PTR, "gx_index_upload: null array");
         if (!d.bA) return fail(GX_ERR_INVLD_PTR, "gx_index_upload: null bA");
         if (d.bA[nbins - 1] != (uint64_t)d.npep * d.speclen)
@@ -149,15 +152,18 @@ extern "C" gx_status gx_index_upload(const gx_length_desc *lens, int32_t nlen, u
     };
     if ((e = cudaMalloc(&ix->bA, sizeof(uint32_t) * (uint64_t)nbins * nlen)) != cudaSuccess ||
         (e = cudaMalloc(&ix->iA, sizeof(uint32_t) * (tot_ia ? tot_ia : 1))) != cudaSuccess ||
-        (e = cudaMalloc(&ix->iAb, sizeof(uint32_t) * (tot_ia ? tot_ia : 1))) != cudaSuccess ||
+        (e = cudaMalloc(&ix->iAb, sizeof(uint16_t) * (tot_ia + 8))) != cudaSuccess ||
         (e = cudaMalloc(&ix->blkA, sizeof(uint32_t) * (tot_blk ? tot_blk : 1))) != cudaSuccess ||
         (e = cudaMalloc(&ix->mass, sizeof(float) * (tot_m ? tot_m : 1))) != cudaSuccess ||
         (e = cudaMalloc(&ix->lens, sizeof(DevLen) * nlen)) != cudaSuccess) {
         cudaGetLastError();
         return cleanup(fail(GX_ERR_BAD_MEM_ALLOC, std::string("gx_index_upload: ") + cudaGetErrorString(e)));
     }
-    ix->bytes = sizeof(uint32_t) * ((uint64_t)nbins * nlen + 2 * tot_ia + tot_blk) + sizeof(float) * tot_m +
-                sizeof(DevLen) * nlen;
+    ix->bytes = sizeof(uint32_t) * ((uint64_t)nbins * nlen + tot_ia + tot_blk) + sizeof(uint16_t) * (tot_ia + 8) +
+                sizeof(float) * tot_m + sizeof(DevLen) * nlen;
+    ix->iab_bytes = sizeof(uint16_t) * tot_ia;
+    if ((e = cudaMemset(ix->iAb + tot_ia, 0, 8 * sizeof(uint16_t))) != cudaSuccess)
+        return cleanup(cuda_fail(e, "gx_index_upload: iAb padding"));
     // scan scratch, sized for the largest per-length offset table
     uint64_t max_rows = 1;
     for (int i = 0; i < nlen; i++) max_rows = std::max<uint64_t>(max_rows, (uint64_t)hl[i].nblk * (nbins + 1));

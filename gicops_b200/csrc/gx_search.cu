@@ -561,7 +561,7 @@ gx_status launch_search(gx_index *ix, gx_workspace *ws, const gx_queries *q, con
     if (q->nspec == 0) return GX_SUCCESS;
     SearchArgs a{};
     a.bA = ix->bA; a.iA = ix->iA; a.iAb = ix->iAb; a.blkA = ix->blkA; a.block = ix->block;
-    a.iab_bytes = 4ull * (ix->hlens.empty() ? 0 : ix->hlens.back().ia_off + (uint64_t)ix->hlens.back().npep * ix->hlens.back().speclen); a.mass = ix->mass; a.lens = ix->lens; a.nlen = ix->nlen; a.nbins = ix->nbins;
+    a.iab_bytes = ix->iab_bytes; a.mass = ix->mass; a.lens = ix->lens; a.nlen = ix->nlen; a.nbins = ix->nbins;
     a.maxz = ix->maxz;
     a.qidx = q->idx; a.moz = q->moz; a.intn = q->intn; a.prec = q->prec; a.dMq = q->dM; a.nspec = q->nspec;
     a.dM = p->dM;
