@@ -164,14 +164,24 @@ __global__ void __launch_bounds__(kPrepBlock) k_prep(SearchArgs a, int2 *win, ui
 // ------------------------------------------------------------------------------------
 // k_search_batched
 // ------------------------------------------------------------------------------------
-constexpr int kBBlock = 1024;
-constexpr int kBWarps = kBBlock / 32;
-constexpr int kPend = 96;       // per-warp queue of candidates awaiting a hyperscore (32 + one scan step)
-constexpr int kIvlChunk = 512;  // intervals per span table
-constexpr int kChunks = 4;      // 16-byte id chunks in flight per lane
+#ifndef GX_BATCH_WARPS
+#define GX_BATCH_WARPS 16
+#endif
+constexpr int kBWarps = GX_BATCH_WARPS;      // warps per CTA
+constexpr int kBBlock = kBWarps * 32;
+constexpr int kCtasPerSm = 1024 / kBBlock;   // resident CTAs per SM (each its own spectrum)
+constexpr int kPend = 160;      // per-warp queue of candidates awaiting a hyperscore (32 + one scan step)
+constexpr int kIvlChunk = 256;  // intervals per span table
+constexpr int kDummy = 32;      // scorecard words that take the adds of ids outside the tile (one per lane)
+#ifndef GX_STREAM_CHUNKS
+#define GX_STREAM_CHUNKS 4
+#endif
+constexpr int kChunks = GX_STREAM_CHUNKS;   // 16-byte id chunks in flight per lane
+constexpr int kHeapWarp = kBWarps - 1;      // inserts heap entrants while the others stream
 constexpr int kEntSmem = 8;     // heap entrants per warp kept in shared memory
 
 // Dynamic shared memory after the scorecard tile (tile * 8 bytes):
+//   dummy      kDummy words right after the scorecard, written and never read
 //   pend       per-warp queue of candidate offsets awaiting a hyperscore
 //   span table of up to kIvlChunk intervals, in the current block of the current length
 //              (element indices relative to the length's 16-byte aligned base):
@@ -185,13 +195,13 @@ struct BatchDyn {
 
 __host__ __device__ constexpr size_t batch_dyn_bytes(int)
 {
-    return sizeof(uint32_t) * ((size_t)kBWarps * kPend + 5 * (size_t)kIvlChunk + (kIvlChunk + 4));
+    return sizeof(uint32_t) * ((size_t)kDummy + (size_t)kBWarps * kPend + 5 * (size_t)kIvlChunk + (kIvlChunk + 4));
 }
 
 __device__ __forceinline__ BatchDyn carve_dyn(unsigned char *base)
 {
     BatchDyn d;
-    uint32_t *p = reinterpret_cast<uint32_t *>(base);
+    uint32_t *p = reinterpret_cast<uint32_t *>(base) + kDummy;
     d.pend = reinterpret_cast<uint32_t (*)[kPend]>(p);
     p += kBWarps * kPend;
     d.sp_q0 = p; p += kIvlChunk;
@@ -224,10 +234,12 @@ struct BatchSmem {
 // id - lo < lim.  Packed scorecard: per candidate a b word and a y word (count << 24 |
 // intensity sum), interleaved, so that id - lo is the word an id adds to; 32-bit adds
 // whose old values are not needed.
-__device__ __forceinline__ void scatter_packed(uint32_t *sc, uint32_t id, uint32_t lo, uint32_t lim, uint32_t vb)
+// Ids outside the tile (or, with ok false, outside the interval) add to the lane's dummy word.
+__device__ __forceinline__ void scatter_packed(uint32_t *sc, uint32_t id, uint32_t lo, uint32_t lim, uint32_t vb,
+                                               uint32_t dummy, bool ok)
 {
     const uint32_t rel = id - lo;
-    if (rel < lim) atomicAdd(sc + rel, vb);
+    atomicAdd(sc + ((rel < lim && ok) ? rel : dummy), vb);
 }
 
 // Wide scorecard (12 bytes): counts b | y << 16, intensity sums of b and y ions.
@@ -243,60 +255,80 @@ __device__ __forceinline__ void scatter_wide(uint32_t *cnt, uint32_t *ib, uint32
     }
 }
 
-// Hyperscores of up to 32 queued candidates (one per lane), in queue order: the
-// histogram and candidate count take every PSM; PSMs with h >= tau go, in order, to
-// the warp's entrant list for the exact heap.
-__device__ __forceinline__ void score_queue(BatchSmem &sm, const BatchDyn &dd, const void *scv, int ctile, int wid,
-                                            int lane, int n, int t0, int ixx, uint32_t speclen, float tau, bool wide,
-                                            Cell *ent, int &nent, int &cps)
+// Hyperscores of the n <= kPend queued candidates of a warp, in queue order: the
+// histogram and candidate count take every PSM; PSMs with h >= tau go, in order, to the
+// warp's entrant list for the exact heap.  Per 64 candidates, all scorecard reads and
+// log10 table loads are issued before any hyperscore is formed.
+__device__ __forceinline__ void score_batch(BatchSmem &sm, const BatchDyn &dd, const SearchArgs &a, const void *scv,
+                                            int ctile, int wid, int lane, int n, int t0, int ixx, uint32_t speclen,
+                                            float tau, bool wide, Cell *ent, int &nent, int &cps)
 {
-    bool psm = false;
-    Cell cell;
-    if (lane < n) {
-        const uint32_t off = dd.pend[wid][lane];
-        uint32_t bc, yc, ib, iy;
-        if (!wide) {
-            const uint2 v = reinterpret_cast<const uint2 *>(scv)[off];
-            bc = v.x >> 24; ib = v.x & 0xFFFFFFu; yc = v.y >> 24; iy = v.y & 0xFFFFFFu;
-        } else {
-            const uint32_t *cnt = reinterpret_cast<const uint32_t *>(scv);
-            const uint32_t cv = cnt[off];
-            bc = cv & 0xFFFFu; yc = cv >> 16;
-            ib = cnt[ctile + off]; iy = cnt[2 * ctile + off];
-        }
-        uint32_t bi = bc, yi = yc;
-        if (bi > 80u || yi > 80u) {
-            atomicOr(&sm.status, 4);
-            bi = min(bi, 80u);
-            yi = min(yi, 80u);
-        }
-        const double h1 = sm.lgf[bi] + sm.lgf[yi];
-        // every lane evaluates both logarithms: no divergence, no table traffic
-        const double lb = log10((double)(1u + ib)), ly = log10((double)(1u + iy));
-        float h = __double2float_rn(h1 + lb + ly - 4.0);
-        if (h > 0.0f) {
-            if (h >= 80.0f) h = 79.0f;
-            psm = true;
-            cell.h = h;
-            cell.psid = t0 + (int)off;
-            cell.ixx = (uint16_t)ixx;
-            cell.shp = (uint16_t)((bc + yc) & 0xFFFFu);
-            cell.total = (uint16_t)speclen;
-            cell.pad = 0;
-            const int hb = __double2int_rz(__dadd_rn((double)__fmul_rn(h, 10.0f), 0.5));
-            atomicAdd(&sm.hist[hb], 1u);
+    constexpr int kG = 2;
+    for (int q0 = 0; q0 < n; q0 += 32 * kG) {
+    uint32_t off[kG], bc[kG], yc[kG], ib[kG], iy[kG];
+    double lb[kG], ly[kG];
+#pragma unroll
+    for (int g = 0; g < kG; g++) {
+        off[g] = 0; bc[g] = yc[g] = ib[g] = iy[g] = 0;
+        if (q0 + 32 * g + lane < n) {
+            off[g] = dd.pend[wid][q0 + 32 * g + lane];
+            if (!wide) {
+                const uint2 v = reinterpret_cast<const uint2 *>(scv)[off[g]];
+                bc[g] = v.x >> 24; ib[g] = v.x & 0xFFFFFFu; yc[g] = v.y >> 24; iy[g] = v.y & 0xFFFFFFu;
+            } else {
+                const uint32_t *cnt = reinterpret_cast<const uint32_t *>(scv);
+                const uint32_t cv = cnt[off[g]];
+                bc[g] = cv & 0xFFFFu; yc[g] = cv >> 16;
+                ib[g] = cnt[ctile + off[g]]; iy[g] = cnt[2 * ctile + off[g]];
+            }
         }
     }
-    const unsigned pb = __ballot_sync(0xffffffffu, psm);
-    cps += __popc(pb);
-    const bool e = psm && cell.h >= tau;
-    const unsigned eb = __ballot_sync(0xffffffffu, e);
-    if (e) {
-        const int g = nent + __popc(eb & ((1u << lane) - 1u));
-        if (g < kEntSmem) sm.ent_s[wid][g] = cell;
-        else ent[g] = cell;
+#pragma unroll
+    for (int g = 0; g < kG; g++) {
+        // log10 of small integers from a table filled by the same log10 (identical values)
+        const uint32_t xb = 1u + ib[g], xy = 1u + iy[g];
+        lb[g] = xb < a.logtab_n ? __ldg(a.logtab + xb) : log10((double)xb);
+        ly[g] = xy < a.logtab_n ? __ldg(a.logtab + xy) : log10((double)xy);
     }
-    nent += __popc(eb);
+#pragma unroll
+    for (int g = 0; g < kG; g++) {
+        if (q0 + 32 * g >= n) break;
+        bool psm = false;
+        Cell cell;
+        if (q0 + 32 * g + lane < n) {
+            uint32_t bi = bc[g], yi = yc[g];
+            if (bi > 80u || yi > 80u) {
+                atomicOr(&sm.status, 4);
+                bi = min(bi, 80u);
+                yi = min(yi, 80u);
+            }
+            const double h1 = sm.lgf[bi] + sm.lgf[yi];
+            float h = __double2float_rn(h1 + lb[g] + ly[g] - 4.0);
+            if (h > 0.0f) {
+                if (h >= 80.0f) h = 79.0f;
+                psm = true;
+                cell.h = h;
+                cell.psid = t0 + (int)off[g];
+                cell.ixx = (uint16_t)ixx;
+                cell.shp = (uint16_t)((bc[g] + yc[g]) & 0xFFFFu);
+                cell.total = (uint16_t)speclen;
+                cell.pad = 0;
+                const int hb = __double2int_rz(__dadd_rn((double)__fmul_rn(h, 10.0f), 0.5));
+                atomicAdd(&sm.hist[hb], 1u);
+            }
+        }
+        const unsigned pb = __ballot_sync(0xffffffffu, psm);
+        cps += __popc(pb);
+        const bool e = psm && cell.h >= tau;
+        const unsigned eb = __ballot_sync(0xffffffffu, e);
+        if (e) {
+            const int gi = nent + __popc(eb & ((1u << lane) - 1u));
+            if (gi < kEntSmem) sm.ent_s[wid][gi] = cell;
+            else ent[gi] = cell;
+        }
+        nent += __popc(eb);
+    }
+    }
 }
 
 // Out-of-line heap insertion (keeps the persistent kernel's register budget for the
@@ -384,13 +416,13 @@ __device__ __forceinline__ void build_span_table(BatchSmem &sm, const BatchDyn &
     if (lane == 31) sm.scan_tmp[wid] = x;
     __syncthreads();
     if (wid == 0) {
-        uint32_t t = sm.scan_tmp[lane];
+        uint32_t t = lane < kBWarps ? sm.scan_tmp[lane] : 0u;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
             if (lane >= o) t += y;
         }
-        sm.scan_tmp[lane] = t;
+        if (lane < kBWarps) sm.scan_tmp[lane] = t;
     }
     __syncthreads();
     const uint32_t incl = x + (wid ? sm.scan_tmp[wid - 1] : 0u);
@@ -408,6 +440,7 @@ __device__ __forceinline__ void stream_tile(BatchSmem &sm, const BatchDyn &dd, c
 {
     const uint32_t M = dd.sp_pre[ncv];
     uint32_t *cnt = reinterpret_cast<uint32_t *>(scv);
+    const uint32_t dummy = 2u * (uint32_t)ctile + (uint32_t)lane;   // packed: words [2T, 2T + 32)
     for (;;) {
         uint32_t u = 0;
         if (lane == 0) u = atomicAdd(&sm.next_unit, 1u);
@@ -444,17 +477,11 @@ __device__ __forceinline__ void stream_tile(BatchSmem &sm, const BatchDyn &dd, c
             const bool full = eq >= a0 && eq + 8u <= a1;
             if (!wide) {
                 const uint32_t vb = (c << 24) | S;
-                if (full) {
 #pragma unroll
-                    for (int m = 0; m < 8; m++)
-                        scatter_packed(cnt, (w4[m >> 1] >> (16 * (m & 1))) & 0xFFFFu, lo, lim, vb);
-                } else {
-#pragma unroll
-                    for (int m = 0; m < 8; m++) {
-                        const uint32_t e = eq + (uint32_t)m;
-                        if (e >= a0 && e < a1)
-                            scatter_packed(cnt, (w4[m >> 1] >> (16 * (m & 1))) & 0xFFFFu, lo, lim, vb);
-                    }
+                for (int m = 0; m < 8; m++) {
+                    const uint32_t e = eq + (uint32_t)m;
+                    scatter_packed(cnt, (w4[m >> 1] >> (16 * (m & 1))) & 0xFFFFu, lo, lim, vb, dummy,
+                                   full || (e >= a0 && e < a1));
                 }
             } else {
 #pragma unroll
@@ -469,7 +496,7 @@ __device__ __forceinline__ void stream_tile(BatchSmem &sm, const BatchDyn &dd, c
     }
 }
 
-__global__ void __launch_bounds__(kBBlock, 1) k_search_batched(SearchArgs a)
+__global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchArgs a)
 {
     extern __shared__ __align__(16) unsigned char dyn[];
     __shared__ BatchSmem sm;
@@ -586,7 +613,9 @@ __global__ void __launch_bounds__(kBBlock, 1) k_search_batched(SearchArgs a)
                         sm.next_unit = 0;
                     __syncthreads();
                     if (heap_due) {          // the previous tile's entrants, off the critical path
-                        if (tid == 0) insert_entrants(sm, a.spill + (uint64_t)blockIdx.x * kBWarps * a.spill_per_warp, a.spill_per_warp, a.heap_cap);
+                        if (wid == kHeapWarp && lane == 0)
+                            insert_entrants(sm, a.spill + (uint64_t)blockIdx.x * kBWarps * a.spill_per_warp,
+                                            a.spill_per_warp, a.heap_cap);
                         heap_due = false;
                     }
                     stream_tile(sm, dd, ia4, ncv, scv, ctile, wide, lo, lim, lane);
@@ -595,56 +624,55 @@ __global__ void __launch_bounds__(kBBlock, 1) k_search_batched(SearchArgs a)
                     __syncthreads();
                 }
                 // ---- scan: warp w owns candidates [w*R, (w+1)*R) and takes them in entry ----
-                // order, two per lane per step (the queue never overflows: 32 + 64 slots),
-                // then clears its range for the next tile
+                // order, four per lane per step, queues those that reach min_shp and scores the
+                // queue when it is full and at the end; then clears its range for the next tile
                 const float tau = sm.heap_size < a.heap_cap ? -1.0f : sm.root;
-                const int step = wide ? 32 : 64;
+                const int step = wide ? 32 : 128;
                 const int R = ((tn + kBWarps - 1) / kBWarps + step - 1) / step * step;
                 const int r0 = min(tn, wid * R), r1 = min(tn, r0 + R);
                 int npend = 0, nent = 0;
                 uint32_t *sw = reinterpret_cast<uint32_t *>(scv);
                 for (int c0 = r0; c0 < r1; c0 += step) {
                     unsigned m = 0;
+                    int cb;
                     if (!wide) {
-                        // lane l: candidates c, c + 1 (c = c0 + 2l), words b, y, b, y
-                        const int c = c0 + 2 * lane;
-                        if (c < r1) {
-                            const uint4 q = *reinterpret_cast<const uint4 *>(sw + 2 * c);
-                            m = ((((q.x >> 24) + (q.y >> 24)) & 0xFFFFu) >= minshp ? 1u : 0u) |
-                                ((((q.z >> 24) + (q.w >> 24)) & 0xFFFFu) >= minshp && c + 1 < r1 ? 2u : 0u);
+                        // lane l: candidates cb .. cb + 3 (cb = c0 + 4l), words b, y, b, y, b, y, b, y
+                        cb = c0 + 4 * lane;
+                        if (cb < r1) {
+                            const uint4 qa = *reinterpret_cast<const uint4 *>(sw + 2 * cb);
+                            const uint4 qb = *reinterpret_cast<const uint4 *>(sw + 2 * cb + 4);
+                            const int lim4 = r1 - cb;   // candidates of the four inside the range
+                            m = ((((qa.x >> 24) + (qa.y >> 24)) >= minshp) ? 1u : 0u) |
+                                ((((qa.z >> 24) + (qa.w >> 24)) >= minshp && lim4 > 1) ? 2u : 0u) |
+                                ((((qb.x >> 24) + (qb.y >> 24)) >= minshp && lim4 > 2) ? 4u : 0u) |
+                                ((((qb.z >> 24) + (qb.w >> 24)) >= minshp && lim4 > 3) ? 8u : 0u);
                         }
                     } else {
-                        const int c = c0 + lane;
-                        if (c < r1) {
-                            const uint32_t cv = sw[c];
+                        cb = c0 + lane;
+                        if (cb < r1) {
+                            const uint32_t cv = sw[cb];
                             m = (((cv & 0xFFFFu) + (cv >> 16)) & 0xFFFFu) >= minshp ? 1u : 0u;
                         }
                     }
-                    // queue positions: lane order, then pair order
+                    // queue positions: lane order, then candidate order inside the lane
                     const unsigned lt = (1u << lane) - 1u;
                     const unsigned B0 = __ballot_sync(0xffffffffu, m & 1u), B1 = __ballot_sync(0xffffffffu, m & 2u);
-                    const int total = __popc(B0) + __popc(B1);
+                    const unsigned B2 = __ballot_sync(0xffffffffu, m & 4u), B3 = __ballot_sync(0xffffffffu, m & 8u);
+                    const int total = __popc(B0) + __popc(B1) + __popc(B2) + __popc(B3);
                     if (total == 0) continue;
-                    int pos = npend + __popc(B0 & lt) + __popc(B1 & lt);
-                    const int cb = wide ? c0 + lane : c0 + 2 * lane;
-                    if (m & 1u) dd.pend[wid][pos++] = (uint32_t)cb;
-                    if (m & 2u) dd.pend[wid][pos] = (uint32_t)(cb + 1);
-                    npend += total;
-                    __syncwarp();
-                    while (npend >= 32) {
-                        score_queue(sm, dd, scv, ctile, wid, lane, 32, t0, ixx, speclen, tau, wide, ent, nent, cps);
+                    if (npend + total > kPend) {   // queue full: score what it holds first
                         __syncwarp();
-                        const uint32_t k0 = lane + 32 < npend ? dd.pend[wid][32 + lane] : 0u;
-                        const uint32_t k1 = lane + 64 < npend ? dd.pend[wid][64 + lane] : 0u;
-                        __syncwarp();
-                        if (lane + 32 < npend) dd.pend[wid][lane] = k0;
-                        if (lane + 64 < npend) dd.pend[wid][32 + lane] = k1;
-                        npend -= 32;
+                        score_batch(sm, dd, a, scv, ctile, wid, lane, npend, t0, ixx, speclen, tau, wide, ent, nent, cps);
+                        npend = 0;
                         __syncwarp();
                     }
+                    int pos = npend + __popc(B0 & lt) + __popc(B1 & lt) + __popc(B2 & lt) + __popc(B3 & lt);
+                    for (unsigned mm = m; mm; mm &= mm - 1u) dd.pend[wid][pos++] = (uint32_t)(cb + __ffs(mm) - 1);
+                    npend += total;
                 }
+                __syncwarp();
                 if (npend > 0)
-                    score_queue(sm, dd, scv, ctile, wid, lane, npend, t0, ixx, speclen, tau, wide, ent, nent, cps);
+                    score_batch(sm, dd, a, scv, ctile, wid, lane, npend, t0, ixx, speclen, tau, wide, ent, nent, cps);
                 if (lane == 0) {
                     sm.warp_cnt[wid] = nent;
                     if (nent) atomicOr(&sm.ent_mask, 1u << wid);
@@ -669,7 +697,7 @@ __global__ void __launch_bounds__(kBBlock, 1) k_search_batched(SearchArgs a)
               }
             }
         }
-        if (heap_due && tid == 0)
+        if (heap_due && wid == kHeapWarp && lane == 0)
             insert_entrants(sm, a.spill + (uint64_t)blockIdx.x * kBWarps * a.spill_per_warp, a.spill_per_warp, a.heap_cap);
         if (lane == 0 && cps) atomicAdd(&sm.cpsms, cps);
         __syncthreads();
@@ -751,6 +779,23 @@ cudaError_t fill_logtab(double *tab, uint32_t n, cudaStream_t st)
 }
 
 size_t batched_dyn_smem(int tile) { return (size_t)tile * 8 + batch_dyn_bytes(tile); }
+
+// CTAs of k_search_batched that fit one SM at this tile size (at most kCtasPerSm).
+int batched_ctas_per_sm(int tile)
+{
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_search_batched, kBBlock, batched_dyn_smem(tile)) !=
+        cudaSuccess)
+        n = 1;
+    return n < 1 ? 1 : (n > kCtasPerSm ? kCtasPerSm : n);
+}
+
+// Largest candidate range of one warp in a tile (its entrants never exceed it).
+uint32_t batched_spill_per_warp(int tile)
+{
+    const int step = 128;
+    return (uint32_t)(((tile + kBWarps - 1) / kBWarps + step - 1) / step * step);
+}
 
 cudaError_t batched_set_attributes(int tile)
 {

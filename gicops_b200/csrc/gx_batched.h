@@ -23,6 +23,8 @@ size_t batched_sort_temp_bytes(uint32_t max_spec);
 cudaError_t fill_logtab(double *tab, uint32_t n, cudaStream_t st);
 constexpr uint32_t kLogTab = 1u << 20;
 cudaError_t batched_set_attributes(int tile);
+int batched_ctas_per_sm(int tile);   // after batched_set_attributes
+uint32_t batched_spill_per_warp(int tile);
 cudaError_t launch_batched(SearchArgs a, const BatchedScratch &b, cudaStream_t st);
 
 }  // namespace gx

@@ -9,7 +9,10 @@
 namespace gx {
 // Entries per block of the block layout; the batched path's scorecard holds one block
 // (8 bytes per entry) and block-local ids 2*entry + 1 must fit 16 bits.
-constexpr int kBlockEntries = 24576;
+#ifndef GX_BLOCK_ENTRIES
+#define GX_BLOCK_ENTRIES 11264
+#endif
+constexpr int kBlockEntries = GX_BLOCK_ENTRIES;
 static_assert(2 * kBlockEntries <= 65536 && kBlockEntries % 32 == 0, "block size");
 }  // namespace gx
 

@@ -501,9 +501,10 @@ extern "C" gx_status gx_workspace_create(const gx_index *ix, uint32_t max_spec, 
         int dev = 0, sms = 0;
         cudaGetDevice(&dev);
         e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        ws->bs.grid = sms;
+        if (e == cudaSuccess) e = batched_set_attributes(ws->tile);
+        ws->bs.grid = sms * batched_ctas_per_sm(ws->tile);
     }
-    ws->spill_per_warp = (uint32_t)((ws->tile + 31) / 32);
+    ws->spill_per_warp = batched_spill_per_warp(ws->tile);
     al((void **)&ws->spill, sizeof(Cell) * (uint64_t)ws->bs.grid * 32 * ws->spill_per_warp);
     al((void **)&ws->logtab, sizeof(double) * kLogTab);
     if (e == cudaSuccess) e = fill_logtab(ws->logtab, kLogTab, nullptr);
