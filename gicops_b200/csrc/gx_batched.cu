@@ -174,7 +174,7 @@ constexpr int kPend = 160;      // per-warp queue of candidates awaiting a hyper
 constexpr int kIvlChunk = 256;  // intervals per span table
 constexpr int kDummy = 32;      // scorecard words that take the adds of ids outside the tile (one per lane)
 #ifndef GX_STREAM_CHUNKS
-#define GX_STREAM_CHUNKS 4
+#define GX_STREAM_CHUNKS 2
 #endif
 constexpr int kChunks = GX_STREAM_CHUNKS;   // 16-byte id chunks in flight per lane
 constexpr int kHeapWarp = kBWarps - 1;      // inserts heap entrants while the others stream
@@ -191,11 +191,12 @@ constexpr int kEntSmem = 8;     // heap entrants per warp kept in shared memory
 struct BatchDyn {
     uint32_t (*pend)[kPend];
     uint32_t *sp_q0, *sp_a0, *sp_a1, *sp_c, *sp_S, *sp_pre;
+    uint32_t *nx_s, *nx_e;   // block offsets of the next tile's intervals
 };
 
 __host__ __device__ constexpr size_t batch_dyn_bytes(int)
 {
-    return sizeof(uint32_t) * ((size_t)kDummy + (size_t)kBWarps * kPend + 5 * (size_t)kIvlChunk + (kIvlChunk + 4));
+    return sizeof(uint32_t) * ((size_t)kDummy + (size_t)kBWarps * kPend + 7 * (size_t)kIvlChunk + (kIvlChunk + 4));
 }
 
 __device__ __forceinline__ BatchDyn carve_dyn(unsigned char *base)
@@ -209,6 +210,8 @@ __device__ __forceinline__ BatchDyn carve_dyn(unsigned char *base)
     d.sp_a1 = p; p += kIvlChunk;
     d.sp_c = p; p += kIvlChunk;
     d.sp_S = p; p += kIvlChunk;
+    d.nx_s = p; p += kIvlChunk;
+    d.nx_e = p; p += kIvlChunk;
     d.sp_pre = p;
     return d;
 }
@@ -227,6 +230,7 @@ struct BatchSmem {
     int32_t spec;
     uint32_t next_unit;
     uint32_t ent_mask;               // warps with entrants in the last scored tile
+    uint32_t ready;                  // the span table of the next tile is built
     float root;
 };
 
@@ -431,6 +435,49 @@ __device__ __forceinline__ void build_span_table(BatchSmem &sm, const BatchDyn &
     if (n == 0 && tid == 0) dd.sp_pre[0] = 0;
 }
 
+// The span table of the next tile, built by one warp from the offsets in nx_s / nx_e
+// while the other warps score (coverage counts and sums of the spectrum's intervals
+// stay in place); it also resets the unit counter.
+__device__ __forceinline__ void build_span_warp(BatchSmem &sm, const BatchDyn &dd, uint32_t n, uint32_t rel0, int lane)
+{
+    constexpr int kPer = kIvlChunk / 32;
+    const uint32_t i0 = (uint32_t)lane * kPer;
+    uint32_t cnt[kPer];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int j = 0; j < kPer; j++) {
+        const uint32_t i = i0 + j;
+        cnt[j] = 0;
+        if (i < n) {
+            const uint32_t a0 = rel0 + dd.nx_s[i], a1 = rel0 + dd.nx_e[i];
+            const uint32_t q0 = a0 >> 3;
+            cnt[j] = a1 > a0 ? ((a1 + 7u) >> 3) - q0 : 0u;
+            dd.sp_q0[i] = q0;
+            dd.sp_a0[i] = a0;
+            dd.sp_a1[i] = a1;
+            sum += cnt[j];
+        }
+    }
+    uint32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    uint32_t run = incl - sum;
+#pragma unroll
+    for (int j = 0; j < kPer; j++) {
+        const uint32_t i = i0 + j;
+        if (i < n) dd.sp_pre[i] = run;
+        run += cnt[j];
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    if (lane == 0) {
+        dd.sp_pre[n] = total;
+        sm.next_unit = 0;
+    }
+}
+
 // Stream the ids of every interval of the span table into the scorecard.  Warps take
 // units of 32 x kChunks consecutive 16-byte chunks (8 ids each) from a shared counter;
 // lane l loads chunks l, l+32, ... of the unit, all before it scatters any.
@@ -520,6 +567,7 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
             sm.status = 0;
             sm.root = 0.0f;
             sm.ent_mask = 0u;
+            sm.ready = 0u;
         }
         for (int i = tid; i < kHist; i += kBBlock) sm.hist[i] = 0;
         __syncthreads();
@@ -586,9 +634,11 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
                   }
               }
               const uint16_t *niA = nullptr;
+              uint32_t nrel0 = 0;
               if (carry && nx >= 0) {
                   const DevLen nl = a.lens[nx];
                   niA = a.iAb + nl.ia_off;
+                  nrel0 = (uint32_t)(nl.ia_off & 7ull);
                   if (tid < (int)nv) {
                       const uint32_t *nbA = a.blkA + nl.blk_off + (uint64_t)nkb * (a.nbins + 1);
                       const Interval v = ivl[tid];
@@ -605,13 +655,16 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
                 if (tn <= 0) continue;
                 const uint32_t lo = 2u * (uint32_t)(t0 - kb * E), lim = 2u * (uint32_t)tn;
                 // ---- stream every interval's ids into the scorecard ----------------------
+                const bool prebuilt = sm.ready != 0u;   // built while the last tile was scored
                 for (uint32_t ic0 = 0; ic0 < nv; ic0 += kIvlChunk) {
                     const uint32_t ncv = min((uint32_t)kIvlChunk, nv - ic0);
-                    if (ti == 0 || nv > (uint32_t)kIvlChunk)
-                        build_span_table(sm, dd, ivl + ic0, ncv, bA, rel0, have, cur_s, cur_e, tid, lane, wid);
-                    else if (tid == 0)
-                        sm.next_unit = 0;
-                    __syncthreads();
+                    if (!prebuilt) {
+                        if (ti == 0 || nv > (uint32_t)kIvlChunk)
+                            build_span_table(sm, dd, ivl + ic0, ncv, bA, rel0, have, cur_s, cur_e, tid, lane, wid);
+                        else if (tid == 0)
+                            sm.next_unit = 0;
+                        __syncthreads();
+                    }
                     if (heap_due) {          // the previous tile's entrants, off the critical path
                         if (wid == kHeapWarp && lane == 0)
                             insert_entrants(sm, a.spill + (uint64_t)blockIdx.x * kBWarps * a.spill_per_warp,
@@ -619,8 +672,11 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
                         heap_due = false;
                     }
                     stream_tile(sm, dd, ia4, ncv, scv, ctile, wide, lo, lim, lane);
-                    if (ti == 0 && niA && tid < (int)nv)   // the next tile's ids into L2
+                    if (ti == 0 && niA && tid < (int)nv) {   // the next tile's ids into L2
                         prefetch_span(a.iAb, a.iab_bytes, niA, nx_s, nx_e);
+                        dd.nx_s[tid] = nx_s;
+                        dd.nx_e[tid] = nx_e;
+                    }
                     __syncthreads();
                 }
                 // ---- scan: warp w owns candidates [w*R, (w+1)*R) and takes them in entry ----
@@ -690,6 +746,17 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
                             uint4 *z = reinterpret_cast<uint4 *>(sw + k * ctile);
                             for (int i = q0 + lane; i < q1; i += 32) z[i] = make_uint4(0u, 0u, 0u, 0u);
                         }
+                    }
+                }
+                // warp 0 prepares the next tile's span table (the others are still scoring)
+                if (wid == 0) {
+                    if (ti + 1 < nsub) {          // next sub-tile of this block: same table
+                        if (lane == 0) { sm.next_unit = 0; sm.ready = 1u; }
+                    } else if (niA) {
+                        build_span_warp(sm, dd, nv, nrel0, lane);
+                        if (lane == 0) sm.ready = 1u;
+                    } else if (lane == 0) {
+                        sm.ready = 0u;
                     }
                 }
                 __syncthreads();
