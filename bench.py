@@ -143,6 +143,9 @@ def main():
     ap.add_argument("--plain", action="store_true", help="time the plain one-spectrum-per-CTA path instead")
     ap.add_argument("--compare-plain", action="store_true", help="also time one step of the plain path")
     ap.add_argument("--spectra", type=int, default=0, help="search only the first N spectra (profiling cases)")
+    ap.add_argument("--no-tail", action="store_true", help="leave the learned tail out of the step")
+    ap.add_argument("--sparse-below", type=int, default=500,
+                    help="queries with fewer candidate PSMs take the learned tail")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -193,9 +196,40 @@ def main():
     t_moz = torch.from_numpy(q.moz.copy()).to(d)
     t_int = torch.from_numpy(q.intn.copy()).to(d)
     t_pre = torch.from_numpy(q.prec.copy()).to(d)
+    t_chg = torch.from_numpy(q.charge.astype(np.int32)).to(d)
     t_out = torch.empty(q.n * N.RESULT_DTYPE.itemsize, dtype=torch.uint8, device=d)
+    t_hist = torch.empty((q.n, N.HIST_BINS), dtype=torch.int32, device=d)
     qd = dict(nspec=q.n, npeaks=len(q.moz), idx=t_idx.data_ptr(), moz=t_moz.data_ptr(), intn=t_int.data_ptr(),
-              prec=t_pre.data_ptr())
+              prec=t_pre.data_ptr(), charge=t_chg.data_ptr())
+
+    # ---- learned tail: trained here (untimed) on this workload's well-populated queries --
+    tail = None
+    tail_info = None
+    if not args.no_tail and not args.plain:
+        import gicops_b200.tail as T
+        t0 = time.perf_counter()
+        ws.search_device(qd, params, t_out.data_ptr(), hist_dev=t_hist.data_ptr(), stream=stream.cuda_stream)
+        torch.cuda.synchronize()
+        res0 = t_out.cpu().numpy().view(N.RESULT_DTYPE)
+        pop = np.nonzero(((res0["status"] & 1) != 0) & (res0["cpsms"] >= 10000) & np.isfinite(res0["slope"]) &
+                         (res0["slope"] < 0))[0]
+        rng = np.random.default_rng(7)
+        pop = rng.permutation(pop)[:4000]
+        tail = T.TailModel(local, max_batch=8192, seed=11)
+        if len(pop) >= 64:
+            dv = dict(hist=t_hist, res=t_out, prec=t_pre, charge=t_chg)
+            smp = T.plan(pop, per_query=32, keep_range=(8, 512), seed=1)
+            xs, ts = T.training_set(tail, dv, res0, smp)
+            tail.set_norm_from(ts.cpu().numpy())
+            losses = tail.train(xs, ts, epochs=6, batch=512, opt=T.Adam(lr=1e-3), seed=2, lr_decay=0.8)
+            tail_info = {"sparse_below": args.sparse_below, "train_queries": int(len(pop)),
+                         "train_samples": int(len(smp)), "train_loss": [round(x, 4) for x in losses],
+                         "train_s": round(time.perf_counter() - t0, 2)}
+            ws.set_tail(tail, args.sparse_below)   # every search below applies it after the plain fit
+        else:
+            tail = None
+        log(f"[bench] learned tail: {tail_info}")
+    del t_hist
 
     def step():
         ws.search_device(qd, params, t_out.data_ptr(), stream=stream.cuda_stream)
@@ -240,9 +274,11 @@ def main():
     top_k = max(kt, key=lambda k: kt[k][1])
     k_ms = kt[top_k][1] / kt[top_k][0]
 
-    # ---- end to end through the host-buffer API ------------------------------------
+    # ---- end to end through the C ABI with host buffers (gx_search_host: pinned host
+    # queries copied in, search, learned tail when attached, results copied out) ------
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
-    qp = gx.synth.QueryBatch(pin(q.idx), pin(q.moz), pin(q.intn), pin(q.prec), pin(q.charge), q.rtime)
+    qp = gx.synth.QueryBatch(pin(q.idx), pin(q.moz), pin(q.intn), pin(q.prec), pin(q.charge.astype(np.int32)),
+                             q.rtime)
     out_pinned = torch.empty(q.n * N.RESULT_DTYPE.itemsize, dtype=torch.uint8).pin_memory().numpy()
     from gicops_b200.search import make_c_queries
     import ctypes as C
@@ -265,7 +301,7 @@ def main():
         t = torch.tensor([e2e_s], device=d)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    h2d = q.idx.nbytes + q.moz.nbytes + q.intn.nbytes + q.prec.nbytes
+    h2d = q.idx.nbytes + q.moz.nbytes + q.intn.nbytes + q.prec.nbytes + 4 * q.n
     d2h = q.n * N.RESULT_DTYPE.itemsize + 4
 
     # ---- roofline numerator: algorithmic bytes of one launch ------------------------
@@ -325,7 +361,10 @@ def main():
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback"},
             "kernel_ms": {k: v[1] / v[0] for k, v in kt.items()},
             "gpu_launches": launches,
-            "path": "plain" if args.plain else "batched",
+            "path": "plain" if args.plain else ("batched+learned tail" if tail else "batched"),
+            "learned_tail": dict(tail_info or {}, queries_replaced=int(
+                ((t_out.cpu().numpy().view(N.RESULT_DTYPE)["status"] & N.STATUS_LEARNED_TAIL) != 0).sum()))
+            if tail else None,
             "plain_path": plain,
             "clocks": summarize_clocks(clocks),
             "cpu_baseline": cpu,

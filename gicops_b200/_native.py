@@ -140,6 +140,7 @@ _SIGS = [
     ("gx_tail_apply", C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                   C.c_uint32, C.c_double, C.c_void_p]),
     ("gx_tail_check", C.c_int32, [C.c_void_p]),
+    ("gx_workspace_set_tail", C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32]),
     ("gx_tail_gemm", C.c_int32, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_int64, C.c_int64, C.c_int32,
                                  C.c_int32, C.c_int32, C.c_void_p, C.c_int64, C.c_void_p]),
     ("gx_last_error", C.c_char_p, []),

@@ -375,6 +375,9 @@ struct gx_workspace {
     int2 *win = nullptr;
     double *lgfact = nullptr;
     int32_t *err = nullptr;
+    // learned tail applied after the tail fit (batched path), when attached
+    gx_tail_model *tail = nullptr;
+    uint32_t tail_below = 0;
     // staging for gx_search_host
     uint32_t *qidx = nullptr;
     int32_t *moz = nullptr, *intn = nullptr, *charge = nullptr;
@@ -558,6 +561,7 @@ gx_status launch_search(gx_index *ix, gx_workspace *ws, const gx_queries *q, con
     int32_t cap;
     gx_status rc = check_params(ix, p, &cap);
     if (rc != GX_SUCCESS) return rc;
+    cudaGetLastError();   // an earlier call's error is not ours to report
     if (q->nspec > ws->max_spec) return fail(GX_ERR_INVLD_SIZE, "more spectra than the workspace holds");
     if (q->nspec == 0) return GX_SUCCESS;
     SearchArgs a{};
@@ -582,6 +586,9 @@ gx_status launch_search(gx_index *ix, gx_workspace *ws, const gx_queries *q, con
         a.spill_per_warp = ws->spill_per_warp;
         cudaError_t e = launch_batched(a, ws->bs, st);
         if (e != cudaSuccess) return cuda_fail(e, "batched search launch");
+        if (ws->tail && ws->tail_below)
+            return gx_tail_apply(ws->tail, a.hist_g, out, q->prec, q->charge, q->nspec, ws->tail_below, p->expect_max,
+                                 st);
         return GX_SUCCESS;
     }
     const uint64_t nw = (uint64_t)q->nspec * ix->nlen;
@@ -600,6 +607,14 @@ gx_status launch_search(gx_index *ix, gx_workspace *ws, const gx_queries *q, con
 }
 
 }  // namespace
+
+extern "C" gx_status gx_workspace_set_tail(gx_workspace *ws, gx_tail_model *m, uint32_t sparse_below)
+{
+    if (!ws) return fail(GX_ERR_INVLD_PTR, "gx_workspace_set_tail: null workspace");
+    ws->tail = m;
+    ws->tail_below = m ? sparse_below : 0u;
+    return GX_SUCCESS;
+}
 
 extern "C" gx_status gx_search_device(gx_index *ix, gx_workspace *ws, const gx_queries *q, const gx_params *p,
                                       gx_result *out, gx_cell *heap, uint32_t *hist, void *stream)
@@ -635,7 +650,8 @@ extern "C" gx_status gx_search_host(gx_index *ix, gx_workspace *ws, const gx_que
     if (q->dM) GX_CUDA(cudaMemcpyAsync(ws->dMq, q->dM, sizeof(double) * n, cudaMemcpyHostToDevice, st));
     gx_queries dq = *q;
     dq.idx = ws->qidx; dq.moz = ws->moz; dq.intn = ws->intn; dq.prec = ws->prec;
-    dq.charge = nullptr;
+    if (q->charge) GX_CUDA(cudaMemcpyAsync(ws->charge, q->charge, sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+    dq.charge = q->charge ? ws->charge : nullptr;
     dq.dM = q->dM ? ws->dMq : nullptr;
     rc = launch_search(ix, ws, &dq, p, ws->out, heap_out ? ws->heap : nullptr, hist_out ? ws->hist : nullptr, st);
     if (rc != GX_SUCCESS) return rc;

@@ -611,6 +611,7 @@ gx_status grads(gx_tail_model *m, const bf16 *X, const float *T, uint32_t n, flo
 gx_status check_model(const gx_tail_model *m, uint32_t n, const char *what)
 {
     if (!m) return fail(GX_ERR_INVLD_PTR, std::string(what) + ": null model");
+    cudaGetLastError();   // an earlier call's error is not ours to report
     if (n > m->max_batch)
         return fail(GX_ERR_INVLD_SIZE, std::string(what) + ": batch of " + std::to_string(n) + " rows exceeds max_batch " +
                                            std::to_string(m->max_batch));
@@ -626,6 +627,7 @@ gx_status check_model(const gx_tail_model *m, uint32_t n, const char *what)
 extern "C" gx_status gx_tail_model_create(int32_t device, uint32_t max_batch, uint64_t seed, gx_tail_model **out)
 {
     if (!out) return fail(GX_ERR_INVLD_PTR, "gx_tail_model_create: null out");
+    cudaGetLastError();
     *out = nullptr;
     if (max_batch == 0 || max_batch > (1u << 22))
         return fail(GX_ERR_INVLD_SIZE, "gx_tail_model_create: max_batch must be in 1..2^22");
@@ -752,6 +754,7 @@ extern "C" gx_status gx_tail_fit_rows(const uint32_t *hist_dev, const int32_t *c
 {
     if (n == 0) return GX_SUCCESS;
     if (!hist_dev || !cpsms_dev || !hyp_dev || !fit_dev) return fail(GX_ERR_INVLD_PTR, "gx_tail_fit_rows: null argument");
+    cudaGetLastError();
     cudaStream_t st = (cudaStream_t)stream;
     int h = prof_begin("k_fit_rows", st);
     k_fit_rows<<<blocks(n, kFitWarps), kFitWarps * 32, 0, st>>>(hist_dev, cpsms_dev, hyp_dev, n, fit_dev);
@@ -854,6 +857,7 @@ extern "C" gx_status gx_tail_gemm(const uint16_t *a_dev, int64_t sam, int64_t sa
                                   int64_t sbk, int32_t M, int32_t N, int32_t K, float *d_dev, int64_t ldd, void *stream)
 {
     if (!a_dev || !b_dev || !d_dev) return fail(GX_ERR_INVLD_PTR, "gx_tail_gemm: null argument");
+    cudaGetLastError();
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cuda_fail(e, "gx_tail_gemm: cudaGetDevice");

@@ -76,6 +76,12 @@ class Searcher:
         except Exception:
             pass
 
+    def set_tail(self, model, sparse_below: int = 500) -> None:
+        """Apply a trained gicops_b200.tail.TailModel to queries with fewer than
+        ``sparse_below`` candidate PSMs in every batched search (None detaches)."""
+        N.check(N.lib().gx_workspace_set_tail(self.handle, model.handle if model else None, sparse_below))
+        self._tail = model   # keep the model alive while attached
+
     def search(self, q: QueryBatch, params: SearchParams, heap: bool = False, hist: bool = False) -> SearchResults:
         """Host buffers in, host results out (H2D, kernels, D2H, synchronise)."""
         n = q.n
@@ -93,10 +99,10 @@ class Searcher:
                       stream: int = 0) -> None:
         """Device buffers (integers: device pointers) already in HBM; stream-ordered, no sync.
 
-        ``q_dev`` holds ``nspec, npeaks, idx, moz, intn, prec`` and optionally ``dM``.
+        ``q_dev`` holds ``nspec, npeaks, idx, moz, intn, prec`` and optionally ``charge``, ``dM``.
         """
         cq = N.Queries(q_dev["nspec"], q_dev["npeaks"], q_dev["idx"], q_dev["moz"], q_dev["intn"], q_dev["prec"],
-                       None, q_dev.get("dM"))
+                       q_dev.get("charge"), q_dev.get("dM"))
         p = params.c()
         N.check(N.lib().gx_search_device(self.index.handle, self.handle, C.byref(cq), C.byref(p), out_dev, heap_dev,
                                          hist_dev, stream))

@@ -135,7 +135,7 @@ typedef struct {
     const int32_t *moz;   /* [npeaks] m/z bins */
     const int32_t *intn;  /* [npeaks] intensities */
     const float *prec;    /* [nspec] precursor masses */
-    const int32_t *charge;/* [nspec] (reported only) */
+    const int32_t *charge;/* [nspec] or NULL (reported; a feature of the learned tail) */
     const double *dM;     /* [nspec] per-spectrum tolerance (Da) or NULL */
 } gx_queries;
 
@@ -298,6 +298,11 @@ gx_status gx_tail_predict(gx_tail_model *m, const uint16_t *x_dev, uint32_t n, f
 gx_status gx_tail_apply(gx_tail_model *m, const uint32_t *hist_dev, gx_result *res_dev, const float *prec_dev,
                         const int32_t *charge_dev, uint32_t nspec, uint32_t sparse_below, double expect_max,
                         void *stream);
+/* Attach a model to a workspace (NULL detaches): every batched search through the
+ * workspace (gx_search_host, gx_search_device) then applies the fallback policy of
+ * gx_tail_apply with sparse_below after the plain fit, on the workspace's stream or the
+ * caller's.  The model must live on the index's device and outlive the attachment. */
+gx_status gx_workspace_set_tail(gx_workspace *ws, gx_tail_model *m, uint32_t sparse_below);
 /* Synchronises and reports a device-side guard of the model's kernels. */
 gx_status gx_tail_check(gx_tail_model *m);
 /* The model's tensor-core GEMM alone: D[M][N] (fp32, row stride ldd) = A * B^T with

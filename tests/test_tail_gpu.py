@@ -195,7 +195,8 @@ def trained(torch):
     m.set_norm_from(t.cpu().numpy())
     losses = m.train(x, t, epochs=15, batch=512, opt=T.Adam(lr=1e-3), seed=2, lr_decay=0.85)
     ev = T.evaluate(m, dv, res, T.plan(held, per_query=4, keep_range=(100, 500), seed=3))
-    return dict(model=m, losses=losses, eval=ev, n_train=len(smp), n_queries=len(ok), dev=dv, res=res)
+    return dict(model=m, losses=losses, eval=ev, n_train=len(smp), n_queries=len(ok), dev=dv, res=res, queries=q,
+                searcher=s)
 
 
 def test_training_reduces_loss(trained):
@@ -253,3 +254,27 @@ def test_fallback_policy_on_search_results(torch, trained):
     assert np.array_equal((out["status"][usable] & 2) != 0, out["e_x"][usable] < 20.0)
     for f in ("slope", "icpt", "e_fp64", "cpsms", "maxhyp"):
         assert np.array_equal(out[f], res0[f]), f
+
+
+def test_workspace_attached_tail_matches_apply(torch, trained):
+    """A model attached to a workspace is applied by gx_search_host after the plain fit,
+    with the same outcome as gx_tail_apply on the detached search's results."""
+    import gicops_b200 as gx
+    import gicops_b200._native as N
+    m, dv, res0 = trained["model"], trained["dev"], trained["res"]
+    q, s = trained["queries"], trained["searcher"]
+    p = gx.SearchParams(dM=500.0, dF=5, topmatches=5, expect_max=20.0)
+    below = int(np.quantile(res0["cpsms"][res0["status"] & 1 > 0], 0.3))
+    plain = s.search(q, p, hist=True)
+    s.set_tail(m, below)
+    try:
+        att = s.search(q, p).result
+    finally:
+        s.set_tail(None)
+    d = torch.device("cuda", 0)
+    res_dev = torch.from_numpy(plain.result.view(np.uint8).copy()).to(d)
+    hist = torch.from_numpy(plain.hist.view(np.int32).copy()).to(d)
+    m.apply(hist, res_dev, dv["prec"], dv["charge"], below, 20.0)
+    ref = res_dev.cpu().numpy().view(N.RESULT_DTYPE)
+    assert ((att["status"] & N.STATUS_LEARNED_TAIL) != 0).sum() > 10
+    assert att.tobytes() == ref.tobytes()
