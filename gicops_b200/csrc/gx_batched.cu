@@ -672,8 +672,7 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
                         heap_due = false;
                     }
                     stream_tile(sm, dd, ia4, ncv, scv, ctile, wide, lo, lim, lane);
-                    if (ti == 0 && niA && tid < (int)nv) {   // the next tile's ids into L2
-                        prefetch_span(a.iAb, a.iab_bytes, niA, nx_s, nx_e);
+                    if (ti == 0 && niA && tid < (int)nv) {   // the next tile's offsets, for its span table
                         dd.nx_s[tid] = nx_s;
                         dd.nx_e[tid] = nx_e;
                     }
