@@ -37,6 +37,7 @@ __global__ void __launch_bounds__(kPrepBlock) k_prep(SearchArgs a, int2 *win, ui
     __shared__ int32_t npk_s;
     __shared__ unsigned long long red[kPrepBlock / 32];
     __shared__ uint32_t nv_s;
+    __shared__ int2 win_s[GX_MAX_LENGTHS];
     const int tid = threadIdx.x;
     const uint32_t s = blockIdx.x;
     if (s >= a.nspec) return;
@@ -124,8 +125,9 @@ __global__ void __launch_bounds__(kPrepBlock) k_prep(SearchArgs a, int2 *win, ui
     unsigned long long vol = 0;
     const uint32_t nv = nv_s;
     const Interval *iv = a.ivl + 2ull * q0;
-    for (int l = 0; l < a.nlen; l++) {
-        const DevLen ln = a.lens[l];
+    // thread l: the window of length l (the binary searches of all lengths run side by side)
+    if (tid < a.nlen) {
+        const DevLen ln = a.lens[tid];
         int lo = 1, hi = 0;
         if (!(dM < 0.0) && ln.npep > 0) {
             const float *m = a.mass + ln.mass_off;
@@ -139,16 +141,24 @@ __global__ void __launch_bounds__(kPrepBlock) k_prep(SearchArgs a, int2 *win, ui
                 hi = (int)x - 1;
             }
         }
-        if (tid == 0) win[(uint64_t)s * a.nlen + l] = make_int2(lo, hi);
-        if (hi >= lo) {
-            const uint32_t W = (uint32_t)(hi - lo + 1);
+        win_s[tid] = make_int2(lo, hi);
+        win[(uint64_t)s * a.nlen + tid] = make_int2(lo, hi);
+    }
+    __syncthreads();
+    // scan volume: ids of every (interval, length) pair with a window, times its tiles
+    const uint32_t npair = nv * (uint32_t)a.nlen;
+#pragma unroll 4
+    for (uint32_t pq = tid; pq < npair; pq += kPrepBlock) {
+        const uint32_t l = pq / nv, i = pq - l * nv;
+        const int2 wv = win_s[l];
+        if (wv.y >= wv.x) {
+            const uint32_t W = (uint32_t)(wv.y - wv.x + 1);
             const uint32_t ntiles = (W + (uint32_t)a.tile - 1) / (uint32_t)a.tile;
             const uint32_t *bA = a.bA + (uint64_t)l * a.nbins;
-            for (uint32_t i = tid; i < nv; i += kPrepBlock)
-                vol += (unsigned long long)(__ldg(bA + iv[i].b1 + 1) - __ldg(bA + iv[i].b0)) * ntiles;
-            if (tid == 0) vol += W;
+            vol += (unsigned long long)(__ldg(bA + iv[i].b1 + 1) - __ldg(bA + iv[i].b0)) * ntiles;
         }
     }
+    if (tid < a.nlen && win_s[tid].y >= win_s[tid].x) vol += (uint32_t)(win_s[tid].y - win_s[tid].x + 1);
     for (int o = 16; o; o >>= 1) vol += __shfl_xor_sync(0xffffffffu, vol, o);
     __syncthreads();
     if ((tid & 31) == 0) red[tid >> 5] = vol;
