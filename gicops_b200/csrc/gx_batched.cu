@@ -822,8 +822,8 @@ __global__ void __launch_bounds__(kTfWarps * 32) k_tailfit(SearchArgs a)
     if ((uint32_t)r.cpsms < a.min_cpsm) return;
     for (int i = lane; i < kHist; i += 32) h[w][i] = a.hist_g[(uint64_t)s * kHist + i];
     __syncwarp();
+    tail_fit_warp(h[w], r.cpsms, r.maxhyp, sx[w], r, lane);
     if (lane == 0) {
-        tail_fit(h[w], r.cpsms, r.maxhyp, sx[w], r);
         r.status |= 1;
         if (r.e_x < a.expect_max) r.status |= 2;
         a.out[s] = r;

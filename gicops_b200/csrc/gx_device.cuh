@@ -237,4 +237,135 @@ __device__ inline void tail_fit(const uint32_t *hist, int32_t cpsms, int32_t hyp
     r.e_fp64 = pow(10.0, mu_t * (double)hyp + beta_t) * (double)(uint32_t)cpsms;
 }
 
+
+// tail_fit with its elementwise steps, integer prefix sums and searches spread over a warp.
+// Bit-identical to tail_fit: prefix sums of integer counts are exact in FP64, every other
+// parallel step is elementwise or a search, and the order-dependent least-squares sums stay
+// in lane 0.  All 32 lanes call it; lane 0 fills r.
+__device__ inline void tail_fit_warp(const uint32_t *hist, int32_t cpsms, int32_t hyp, double *sx_buf, gx_result &r,
+                                     int lane)
+{
+    constexpr unsigned kAll = 0xffffffffu;
+    constexpr int kNone = 0x7fffffff;
+    int e = -1;
+    for (int p = hyp - 1 - lane; p >= 0; p -= 32)
+        if (hist[p] >= 1u) { e = p; break; }
+    for (int o = 16; o; o >>= 1) e = max(e, __shfl_xor_sync(kAll, e, o));
+    int end1 = e >= 0 ? e : hyp - 1;
+    int st = kNone;
+    for (int p = lane; p <= end1; p += 32)
+        if (hist[p] >= 1u) { st = p; break; }
+    for (int o = 16; o; o >>= 1) st = min(st, __shfl_xor_sync(kAll, st, o));
+    const int stt1 = st == kNone ? 0 : st;
+    if (stt1 == end1) end1 += 1;
+    double mu_t = 0.0, beta_t = 4.0;
+    if (cpsms < 1) {
+        mu_t = 0.0;
+        beta_t = 100.0;
+    } else {
+        if (lane == 0) sx_buf[0] = 0.0;  // the element before the slice (read when mark == -1)
+        double *sx = sx_buf + 1;
+        const int size = max(0, end1 - stt1 + 1);
+        // cumulative counts: lane l sums a contiguous run, then a warp scan
+        const int per = (size + 31) / 32;
+        const int b0 = min(size, lane * per), b1 = min(size, b0 + per);
+        unsigned long long part = 0;
+        for (int i = b0; i < b1; i++) part += hist[stt1 + i];
+        unsigned long long incl = part;
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long y = __shfl_up_sync(kAll, incl, o);
+            if (lane >= o) incl += y;
+        }
+        unsigned long long run = incl - part;
+        for (int i = b0; i < b1; i++) {
+            run += hist[stt1 + i];
+            sx[i] = (double)run;
+        }
+        __syncwarp();
+        for (int i = lane; i < size; i += 32) {
+            double v = sx[i] / (double)cpsms;
+            v = v + (-1.0);
+            sx[i] = -v;
+            if (sx[i] > 1.0) sx[i] = 0.999;
+        }
+        __syncwarp();
+        if (size > 0) {
+            int rp = -1;
+            for (int p = size - 1 - lane; p >= 0; p -= 32)
+                if (sx[p] >= 1e-4) { rp = p; break; }
+            for (int o = 16; o; o >>= 1) rp = max(rp, __shfl_xor_sync(kAll, rp, o));
+            const double v = sx[rp >= 0 ? rp : size - 1];
+            __syncwarp();
+            for (int i = lane; i < size; i += 32)
+                if (sx[i] <= 0.0) sx[i] = v;
+        }
+        __syncwarp();
+        for (int i = lane; i < size; i += 32) sx[i] = log10(sx[i]);
+        __syncwarp();
+        int mark = 0, mark2 = 0;
+        if (size >= 3) {
+            const double hgt = sx[size - 1] - sx[0];
+            const double t22 = sx[0] + hgt * 0.22;
+            int lm = kNone;
+            for (int p = lane; p < size; p += 32)
+                if (sx[p] <= t22) { lm = p; break; }
+            for (int o = 16; o; o >>= 1) lm = min(lm, __shfl_xor_sync(kAll, lm, o));
+            mark = (lm == kNone ? 0 : lm) - 1;
+            mark2 = size - 1;
+            if (size > 3) {
+                const double t87 = sx[0] + hgt * 0.87;
+                int m2 = -1;
+                for (int p = size - 1 - lane; p >= 0; p -= 32)
+                    if (sx[p] >= t87) { m2 = p; break; }
+                for (int o = 16; o; o >>= 1) m2 = max(m2, __shfl_xor_sync(kAll, m2, o));
+                if (m2 >= 0) mark2 = m2;
+            }
+            if (mark >= mark2) mark = mark2 - 1;
+        } else {
+            mark = 0;
+            mark2 = size - 1;
+        }
+        const int n = mark2 - mark + 1;
+        if (lane == 0) {
+            if (n == 1) {
+                mu_t = 0.0;
+                beta_t = sx[mark];
+            } else if (n >= 2) {
+                double xbar = 0.0, ybar = 0.0;
+                for (int i = 0; i < n; i++) {
+                    xbar = xbar + (double)(stt1 + mark + i);
+                    ybar = ybar + sx[mark + i];
+                }
+                xbar = xbar / (double)n;
+                ybar = ybar / (double)n;
+                double top = 0.0, bot = 0.0;
+                for (int i = 0; i < n; i++) {
+                    const double dx = (double)(stt1 + mark + i) - xbar;
+                    top = top + dx * (sx[mark + i] - ybar);
+                    bot = bot + dx * dx;
+                }
+                mu_t = top / bot;
+                beta_t = ybar - mu_t * xbar;
+            } else {
+                mu_t = __longlong_as_double(0x7ff8000000000000ll);
+                beta_t = mu_t;
+            }
+        }
+    }
+    if (lane == 0) {
+        r.slope = mu_t;
+        r.icpt = beta_t;
+        r.mu = to_int_x86(mu_t * 1e6);
+        r.beta = to_int_x86(beta_t * 1e6);
+        r.stt1 = stt1;
+        r.end1 = end1;
+        double w = (double)r.mu, b = (double)r.beta;
+        w /= 1e6;
+        b /= 1e6;
+        const double lgs = (w * (double)hyp) + b;
+        r.e_x = pow(10.0, lgs) * (double)(uint32_t)cpsms;
+        r.e_fp64 = pow(10.0, mu_t * (double)hyp + beta_t) * (double)(uint32_t)cpsms;
+    }
+}
+
 }  // namespace gx
