@@ -5,10 +5,11 @@
 //                   merged into disjoint bin intervals (coverage count, intensity sum),
 //                   the packed-scorecard guard and the scan volume (sort key)
 //   (radix sort of the spectra by scan volume, descending)
-//   k_search_batched  persistent CTAs; per spectrum, per length, per candidate tile:
-//                   stream the iA span of every interval (each bucket read once),
-//                   accumulate the BYC scorecard in shared memory, then scan the tile
-//                   in entry order (hyperscore, histogram, exact top-K heap)
+//   k_search_batched  persistent CTAs (two per SM); per spectrum, per length, per
+//                   candidate tile (one block of the block layout): stream the 16-bit ids
+//                   of every interval (each bucket read once) into the BYC scorecard in
+//                   shared memory, then scan the tile in entry order (hyperscore,
+//                   histogram, exact top-K heap)
 //   k_tailfit       one warp per spectrum: expeRT tail fit and e-value
 //
 // Results are identical to the reference's CPU path (source/core/dslim_query.cpp:
@@ -354,21 +355,6 @@ __device__ __noinline__ void heap_insert_many(Cell *heap, int *size, int cap, co
     *size = hs;
 }
 
-// Bring the ids [st, en) (element indices) of a block into L2 ahead of its tile: one bulk
-// prefetch per span, rounded out to 16-byte boundaries inside the iAb allocation.
-__device__ __forceinline__ void prefetch_span(const uint16_t *iAb_base, uint64_t iab_bytes, const uint16_t *iA,
-                                              uint32_t st, uint32_t en)
-{
-    if (en <= st) return;
-    const uint64_t base = reinterpret_cast<uint64_t>(iAb_base);
-    uint64_t lo = reinterpret_cast<uint64_t>(iA + st) & ~15ull;
-    uint64_t hi = (reinterpret_cast<uint64_t>(iA + en) + 15ull) & ~15ull;
-    const uint64_t end = (base + iab_bytes) & ~15ull;
-    if (hi > end) hi = end;
-    if (lo < base || hi <= lo) return;
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(lo), "r"((uint32_t)(hi - lo)) : "memory");
-}
-
 // Thread 0 inserts the entrants of the warps that have some (in warp order) of the last
 // scored tile: the first few of each warp from shared memory, any overflow from the
 // warp's global spill.
@@ -602,8 +588,8 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
         int cps = 0;   // candidate PSMs counted by this warp (lane 0 adds them at the end)
         bool heap_due = false;
         // Offsets of the next tile's bins, loaded by thread i for interval i one tile ahead
-        // (when all intervals fit one span table): they feed the L2 prefetch of that tile's
-        // ids and its span table.
+        // (when all intervals fit one span table): warp 0 builds that tile's span table from
+        // them while the others score.
         uint32_t nx_s = 0, nx_e = 0;
         int nx_len = -1;
         int64_t nx_kb = -1;
