@@ -346,42 +346,58 @@ __device__ __forceinline__ void score_batch(BatchSmem &sm, const BatchDyn &dd, c
     }
 }
 
-// Out-of-line heap insertion (keeps the persistent kernel's register budget for the
-// streaming loop).
-__device__ __noinline__ void heap_insert_many(Cell *heap, int *size, int cap, const Cell *cells, int n)
-{
-    int hs = *size;
-    for (int k = 0; k < n; k++) heap_insert(heap, hs, cap, cells[k]);
-    *size = hs;
-}
-
-// Thread 0 inserts the entrants of the warps that have some (in warp order) of the last
-// scored tile: the first few of each warp from shared memory, any overflow from the
-// warp's global spill.
-__device__ __noinline__ void insert_entrants(BatchSmem &sm, const Cell *spill_cta, uint32_t spill_per_warp, int cap)
+// Warp kHeapWarp inserts the entrants of the warps that have some (in warp order) of the
+// last scored tile into the heap, in the order a single thread would: the first few of
+// each warp from shared memory, any overflow from the warp's global spill.  The warp loads
+// 32 entrants at a time (the next 32 in flight while these are inserted); once the heap is
+// full, a cell below its root is rejected by heap_insert and the root never decreases, so
+// the lanes drop the cells below the root at the start of the batch and lane 0 inserts
+// only the others.  Every lane tracks the heap size (an insertion into a heap that is not
+// full always appends).
+__device__ __noinline__ void insert_entrants(BatchSmem &sm, const Cell *spill_cta, uint32_t spill_per_warp, int cap,
+                                             int lane)
 {
     int hs = sm.heap_size;
-    for (uint32_t mask = sm.ent_mask; mask; mask &= mask - 1u) {
+    const uint32_t mask0 = sm.ent_mask;
+    for (uint32_t mask = mask0; mask; mask &= mask - 1u) {
         const int w2 = __ffs(mask) - 1;
         const int n2 = sm.warp_cnt[w2];
-        const int ns = min(n2, kEntSmem);
-        for (int k = 0; k < ns; k++) heap_insert(sm.heap, hs, cap, sm.ent_s[w2][k]);
-        if (n2 > kEntSmem) {
-            sm.heap_size = hs;
-            const Cell *e2 = spill_cta + (uint64_t)w2 * spill_per_warp;
-            for (int k0 = kEntSmem; k0 < n2; k0 += 8) {
-                Cell c8[8];
-#pragma unroll
-                for (int k = 0; k < 8; k++)
-                    if (k0 + k < n2) c8[k] = e2[k0 + k];
-                heap_insert_many(sm.heap, &sm.heap_size, cap, c8, min(8, n2 - k0));
+        const Cell *e2 = spill_cta + (uint64_t)w2 * spill_per_warp;
+        Cell nxt;
+        if (lane < n2) nxt = lane < kEntSmem ? sm.ent_s[w2][lane] : e2[lane];
+        for (int k0 = 0; k0 < n2; k0 += 32) {
+            const Cell c = nxt;
+            const bool v = k0 + lane < n2;
+            const int k1 = k0 + 32 + lane;
+            if (k1 < n2) nxt = e2[k1];
+            __syncwarp();
+            const float root = hs == cap ? sm.heap[0].h : -INFINITY;
+            uint32_t live = __ballot_sync(0xffffffffu, v && c.h >= root);
+            const uint32_t u1 = ((uint32_t)c.ixx) | ((uint32_t)c.shp << 16);
+            const uint32_t u2 = ((uint32_t)c.total) | ((uint32_t)c.pad << 16);
+            while (live) {
+                const int j = __ffs(live) - 1;
+                live &= live - 1u;
+                Cell cj;
+                cj.h = __shfl_sync(0xffffffffu, c.h, j);
+                cj.psid = __shfl_sync(0xffffffffu, c.psid, j);
+                const uint32_t v1 = __shfl_sync(0xffffffffu, u1, j), v2 = __shfl_sync(0xffffffffu, u2, j);
+                cj.ixx = (uint16_t)(v1 & 0xFFFFu); cj.shp = (uint16_t)(v1 >> 16);
+                cj.total = (uint16_t)(v2 & 0xFFFFu); cj.pad = (uint16_t)(v2 >> 16);
+                if (lane == 0) {
+                    int h0 = hs;
+                    heap_insert(sm.heap, h0, cap, cj);
+                }
+                hs = min(hs + 1, cap);
             }
-            hs = sm.heap_size;
         }
     }
-    sm.heap_size = hs;
-    sm.root = sm.heap[0].h;
-    sm.ent_mask = 0u;
+    __syncwarp();
+    if (lane == 0) {
+        sm.heap_size = hs;
+        sm.root = sm.heap[0].h;
+        sm.ent_mask = 0u;
+    }
 }
 
 // Span table of up to kIvlChunk intervals for one block of one length (element indices
@@ -662,9 +678,9 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
                         __syncthreads();
                     }
                     if (heap_due) {          // the previous tile's entrants, off the critical path
-                        if (wid == kHeapWarp && lane == 0)
+                        if (wid == kHeapWarp)
                             insert_entrants(sm, a.spill + (uint64_t)blockIdx.x * kBWarps * a.spill_per_warp,
-                                            a.spill_per_warp, a.heap_cap);
+                                            a.spill_per_warp, a.heap_cap, lane);
                         heap_due = false;
                     }
                     stream_tile(sm, dd, ia4, ncv, scv, ctile, wide, lo, lim, lane);
@@ -759,8 +775,9 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
               }
             }
         }
-        if (heap_due && wid == kHeapWarp && lane == 0)
-            insert_entrants(sm, a.spill + (uint64_t)blockIdx.x * kBWarps * a.spill_per_warp, a.spill_per_warp, a.heap_cap);
+        if (heap_due && wid == kHeapWarp)
+            insert_entrants(sm, a.spill + (uint64_t)blockIdx.x * kBWarps * a.spill_per_warp, a.spill_per_warp, a.heap_cap,
+                            lane);
         if (lane == 0 && cps) atomicAdd(&sm.cpsms, cps);
         __syncthreads();
         // ---- per-spectrum outputs (the tail fit runs in k_tailfit) -------------------
@@ -780,7 +797,7 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
             memset(&r, 0, sizeof(r));
             r.cpsms = sm.cpsms;
             r.status = sm.status;
-            if ((uint32_t)sm.cpsms >= a.min_cpsm) {
+            if (fits_tail(sm.cpsms, a.min_cpsm)) {
                 const Cell t = heap_getmax(sm.heap, sm.heap_size);
                 r.top.hyperscore = t.h; r.top.psid = t.psid; r.top.idxoffset = t.ixx;
                 r.top.sharedions = t.shp; r.top.totalions = t.total;
@@ -805,7 +822,7 @@ __global__ void __launch_bounds__(kTfWarps * 32) k_tailfit(SearchArgs a)
     const uint32_t s = blockIdx.x * kTfWarps + w;
     if (s >= a.nspec) return;
     gx_result r = a.out[s];
-    if ((uint32_t)r.cpsms < a.min_cpsm) return;
+    if (!fits_tail(r.cpsms, a.min_cpsm)) return;
     for (int i = lane; i < kHist; i += 32) h[w][i] = a.hist_g[(uint64_t)s * kHist + i];
     __syncwarp();
     tail_fit_warp(h[w], r.cpsms, r.maxhyp, sx[w], r, lane);

@@ -58,7 +58,7 @@ struct SearchArgs {
                           // block-local ids 2*(entry - block start) + (y ion)
     const uint32_t *blkA; // block layout offsets [nblk][nbins + 1] per length (relative to ia_off)
     uint32_t block;       // entries per block
-    uint64_t iab_bytes;   // bytes of ids in iAb (bounds the L2 prefetches)
+    uint64_t iab_bytes;   // bytes of ids in iAb (the allocation adds one 16-byte chunk)
     const float *mass;
     const DevLen *lens;
     int32_t nlen;
@@ -129,6 +129,13 @@ __device__ __forceinline__ void heap_insert(Cell *a, int &size, int cap, const C
     }
     a[size++] = c;
     for (int i = (size - 1) / 2; i >= 0; i--) heap_sift(a, size, i);
+}
+
+// A spectrum gets an e-value when it has at least min_cpsm candidate PSMs and at least one
+// (min_cpsm 0 acts as 1: with no candidate PSM the heap is empty and there is no top score).
+__device__ __forceinline__ bool fits_tail(int32_t cpsms, uint32_t min_cpsm)
+{
+    return cpsms > 0 && (uint32_t)cpsms >= min_cpsm;
 }
 
 __device__ __forceinline__ Cell heap_getmax(const Cell *a, int size)

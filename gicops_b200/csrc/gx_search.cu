@@ -344,7 +344,7 @@ __global__ void __launch_bounds__(kBlock) k_search_plain(SearchArgs a, int tile)
         memset(&r, 0, sizeof(r));
         r.cpsms = sm.cpsms;
         int st = sm.status;
-        if ((uint32_t)sm.cpsms >= a.min_cpsm) {
+        if (fits_tail(sm.cpsms, a.min_cpsm)) {
             st |= 1;
             const Cell t = heap_getmax(sm.heap, sm.heap_size);
             r.top.hyperscore = t.h; r.top.psid = t.psid; r.top.idxoffset = t.ixx;

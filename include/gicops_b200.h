@@ -118,7 +118,8 @@ typedef struct {
     uint32_t scale;       /* bins per Da */
     double max_mass;      /* Da */
     uint32_t min_shp;     /* shared peaks for a candidate PSM (4) */
-    uint32_t min_cpsm;    /* candidate PSMs for an e-value (4) */
+    uint32_t min_cpsm;    /* candidate PSMs for an e-value (4); 0 acts as 1 (an e-value needs a
+                           * top PSM; the reference reads its empty heap there) */
     uint32_t topmatches;  /* heap capacity = 2^floor(log2(t)+0.999) - 1 (dslim.cpp:438-444) */
     uint32_t flags;       /* GX_FLAG_* */
     double expect_max;    /* PSMs with e >= expect_max are not reported */
@@ -149,7 +150,7 @@ typedef struct {
     uint16_t pad;
 } gx_cell;
 
-/* Per-spectrum result.  status bits: 1 = cpsms >= min_cpsm (e-value computed),
+/* Per-spectrum result.  status bits: 1 = cpsms >= max(min_cpsm, 1) (e-value computed),
  * 2 = e_x < expect_max (a PSM the reference prints), 4 = a shared-ion count above
  * MAX_SHDPEAKS (80) was clamped, 8 = the 12-byte scorecard was used, 16 = the e-value
  * comes from the learned tail (gx_tail_apply). */

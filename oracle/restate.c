@@ -289,7 +289,7 @@ static void search_one(const rs_length *lens, int nlen, const int32_t *moz, cons
     res->cpsms = (int32_t)cpsms;
     res->heap_size = heap.size;
     memcpy(res->heap, heap.a, sizeof(rs_cell) * (size_t)heap.size);
-    if (cpsms >= par->min_cpsm) {
+    if (cpsms > 0 && cpsms >= par->min_cpsm) {   /* min_cpsm 0 acts as 1: an empty heap has no top */
         status |= 1;
         res->top = heap_getmax(&heap);
         res->maxhyp = (int32_t)((double)(res->top.hyperscore * 10.0f) + 0.5);

@@ -151,3 +151,22 @@ def test_gpu_errors_are_status_codes(gx, golden):
     # the context stays usable afterwards
     r = s.search(q.subset([0, 1]), search_params(c))
     assert r.result.shape == (2,)
+
+
+@pytest.mark.parametrize("flags", [0, 1, 2], ids=["default", "wide", "plain"])
+def test_gpu_min_cpsm_zero_and_one(gx, golden, flags):
+    """min_cpsm 0 acts as 1: spectra that probe bins but get no candidate PSM (a high
+    shared-peak threshold) have no e-value; the rest are fitted as usual."""
+    c = golden("open_mox")
+    H, q = c["index"], c["queries"]
+    dev = gx.DeviceIndex(H, 0)
+    s = gx.Searcher(dev, q.n, len(q.moz))
+    for mc in (0, 1):
+        p = gx.SearchParams(dM=500.0, min_shp=16, min_cpsm=mc, expect_max=1e300, flags=flags)
+        r = s.search(q, p, heap=True, hist=True)
+        ores, ohist = pyoracle.search(H.lengths, q, pyoracle.Params(dM=500.0, min_shp=16, min_cpsm=mc), hist=True)
+        assert_same(r.result, r.heap, r.hist, ores, ohist, None)
+        none = r.result["cpsms"] == 0
+        assert none.sum() > 0 and (~none).sum() > 0
+        assert np.all((r.result["status"][none] & 1) == 0)
+        assert np.all((r.result["status"][~none] & 1) != 0)

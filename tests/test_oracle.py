@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 import pyoracle
-from conftest import CASES, oracle_params
+from conftest import CASES, case_index, case_queries, load_case, oracle_params
 
 
 @pytest.mark.parametrize("case", CASES)
@@ -127,3 +127,14 @@ def test_tailfit_short_branches():
     assert r["mu"] == int(r["slope"] * 1e6)
     e = 10 * 10 ** ((r["mu"] / 1e6) * 30 + r["beta"] / 1e6)
     assert r["e_x"] == pytest.approx(e, rel=1e-12)
+
+
+def test_oracle_min_cpsm_zero_acts_as_one():
+    """A spectrum without candidate PSMs has no top score, so no e-value even at min_cpsm 0."""
+    c = load_case("open_mox")
+    H, q = case_index(c), case_queries(c)
+    a, ha = pyoracle.search(H.lengths, q, pyoracle.Params(dM=500.0, min_shp=16, min_cpsm=0), hist=True)
+    b, hb = pyoracle.search(H.lengths, q, pyoracle.Params(dM=500.0, min_shp=16, min_cpsm=1), hist=True)
+    assert a.tobytes() == b.tobytes() and np.array_equal(ha, hb)
+    none = a["cpsms"] == 0
+    assert none.sum() > 10 and np.all(a["status"][none] == 0) and np.all((a["status"][~none] & 1) != 0)
