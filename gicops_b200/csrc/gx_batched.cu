@@ -195,13 +195,16 @@ constexpr int kEntSmem = 8;     // heap entrants per warp kept in shared memory
 //   dummy      kDummy words right after the scorecard, written and never read
 //   pend       per-warp queue of candidate offsets awaiting a hyperscore
 //   span table of up to kIvlChunk intervals, in the current block of the current length
-//              (element indices relative to the length's 16-byte aligned base):
-//              q0 = 16-byte chunk of the first id, [a0, a1) = the interval's ids,
-//              c, S = coverage count and intensity sum, pre = exclusive prefix of the
-//              intervals' chunk counts (kIvlChunk + 1)
+//              (element indices relative to the length's 16-byte aligned base), one
+//              16-byte record per interval: x = q0 - pre (q0 = 16-byte chunk of the first
+//              id, so that chunk j of the table is x + j), [y, z) = the interval's ids,
+//              w = the add of one id (packed: c << 24 | S; wide: S), with c, S the
+//              coverage count and intensity sum; sp_c = c (wide scorecard); pre =
+//              exclusive prefix of the intervals' chunk counts (kIvlChunk + 1)
 struct BatchDyn {
     uint32_t (*pend)[kPend];
-    uint32_t *sp_q0, *sp_a0, *sp_a1, *sp_c, *sp_S, *sp_pre;
+    uint4 *sp_rec;
+    uint32_t *sp_c, *sp_pre;
     uint32_t *nx_s, *nx_e;   // block offsets of the next tile's intervals
 };
 
@@ -216,11 +219,8 @@ __device__ __forceinline__ BatchDyn carve_dyn(unsigned char *base)
     uint32_t *p = reinterpret_cast<uint32_t *>(base) + kDummy;
     d.pend = reinterpret_cast<uint32_t (*)[kPend]>(p);
     p += kBWarps * kPend;
-    d.sp_q0 = p; p += kIvlChunk;
-    d.sp_a0 = p; p += kIvlChunk;
-    d.sp_a1 = p; p += kIvlChunk;
+    d.sp_rec = reinterpret_cast<uint4 *>(p); p += 4 * kIvlChunk;   // 16-byte aligned (see batch_dyn_bytes)
     d.sp_c = p; p += kIvlChunk;
-    d.sp_S = p; p += kIvlChunk;
     d.nx_s = p; p += kIvlChunk;
     d.nx_e = p; p += kIvlChunk;
     d.sp_pre = p;
@@ -243,6 +243,10 @@ struct BatchSmem {
     uint32_t ent_mask;               // warps with entrants in the last scored tile
     uint32_t ready;                  // the span table of the next tile is built
     float root;
+    // keep masks of a 16-byte chunk's eight ids: keep_lo[m] keeps ids m.., keep_hi[m]
+    // keeps ids ..m (index m - 1)
+    uint4 keep_lo[8];
+    uint4 keep_hi[8];
 };
 
 // Block-local ids are 2*(entry - block start) + (y ion); the tile's ids satisfy
@@ -406,20 +410,19 @@ __device__ __noinline__ void insert_entrants(BatchSmem &sm, const Cell *spill_ct
 // already holds the block offsets of interval i (loaded one tile ahead).
 __device__ __forceinline__ void build_span_table(BatchSmem &sm, const BatchDyn &dd, const Interval *iv, uint32_t n,
                                                  const uint32_t *__restrict__ bA, uint32_t rel0, bool have,
-                                                 uint32_t have_s, uint32_t have_e, int tid, int lane, int wid)
+                                                 uint32_t have_s, uint32_t have_e, bool wide, int tid, int lane,
+                                                 int wid)
 {
-    uint32_t cnt = 0;
+    uint32_t cnt = 0, rq0 = 0;
     if (tid < (int)n) {
         const Interval v = iv[tid];
         const uint32_t a0 = rel0 + (have ? have_s : __ldg(bA + v.b0));
         const uint32_t a1 = rel0 + (have ? have_e : __ldg(bA + v.b1 + 1));
         const uint32_t q0 = a0 >> 3;
         cnt = a1 > a0 ? ((a1 + 7u) >> 3) - q0 : 0u;
-        dd.sp_q0[tid] = q0;
-        dd.sp_a0[tid] = a0;
-        dd.sp_a1[tid] = a1;
+        rq0 = q0;
+        dd.sp_rec[tid] = make_uint4(0u, a0, a1, wide ? v.S : ((v.c << 24) | v.S));
         dd.sp_c[tid] = v.c;
-        dd.sp_S[tid] = v.S;
     }
     if (tid == 0) sm.next_unit = 0;
     // block exclusive scan of cnt
@@ -442,31 +445,35 @@ __device__ __forceinline__ void build_span_table(BatchSmem &sm, const BatchDyn &
     }
     __syncthreads();
     const uint32_t incl = x + (wid ? sm.scan_tmp[wid - 1] : 0u);
-    if (tid < (int)n) dd.sp_pre[tid] = incl - cnt;
+    if (tid < (int)n) {
+        dd.sp_pre[tid] = incl - cnt;
+        dd.sp_rec[tid].x = rq0 - (incl - cnt);
+    }
     if (tid == (int)n - 1) dd.sp_pre[n] = incl;
     if (n == 0 && tid == 0) dd.sp_pre[0] = 0;
 }
 
 // The span table of the next tile, built by one warp from the offsets in nx_s / nx_e
-// while the other warps score (coverage counts and sums of the spectrum's intervals
-// stay in place); it also resets the unit counter.
+// while the other warps score (the adds of the spectrum's intervals, record field w and
+// sp_c, stay in place); it also resets the unit counter.
 __device__ __forceinline__ void build_span_warp(BatchSmem &sm, const BatchDyn &dd, uint32_t n, uint32_t rel0, int lane)
 {
     constexpr int kPer = kIvlChunk / 32;
     const uint32_t i0 = (uint32_t)lane * kPer;
-    uint32_t cnt[kPer];
+    uint32_t cnt[kPer], q0s[kPer];
     uint32_t sum = 0;
 #pragma unroll
     for (int j = 0; j < kPer; j++) {
         const uint32_t i = i0 + j;
         cnt[j] = 0;
+        q0s[j] = 0;
         if (i < n) {
             const uint32_t a0 = rel0 + dd.nx_s[i], a1 = rel0 + dd.nx_e[i];
             const uint32_t q0 = a0 >> 3;
             cnt[j] = a1 > a0 ? ((a1 + 7u) >> 3) - q0 : 0u;
-            dd.sp_q0[i] = q0;
-            dd.sp_a0[i] = a0;
-            dd.sp_a1[i] = a1;
+            q0s[j] = q0;
+            dd.sp_rec[i].y = a0;
+            dd.sp_rec[i].z = a1;
             sum += cnt[j];
         }
     }
@@ -480,7 +487,10 @@ __device__ __forceinline__ void build_span_warp(BatchSmem &sm, const BatchDyn &d
 #pragma unroll
     for (int j = 0; j < kPer; j++) {
         const uint32_t i = i0 + j;
-        if (i < n) dd.sp_pre[i] = run;
+        if (i < n) {
+            dd.sp_pre[i] = run;
+            dd.sp_rec[i].x = q0s[j] - run;
+        }
         run += cnt[j];
     }
     const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
@@ -492,14 +502,20 @@ __device__ __forceinline__ void build_span_warp(BatchSmem &sm, const BatchDyn &d
 
 // Stream the ids of every interval of the span table into the scorecard.  Warps take
 // units of 32 x kChunks consecutive 16-byte chunks (8 ids each) from a shared counter;
-// lane l loads chunks l, l+32, ... of the unit, all before it scatters any.
+// lane l loads chunks l, l+32, ... of the unit, all before it scatters any.  The ids of
+// a chunk outside its interval (at most the first and last chunk of an interval have
+// some) are replaced through the keep masks: with the lane's dummy word when the tile
+// is a whole block (every id of the block is then a word of the tile and needs no
+// range check), else with 0xFFFF, which the range check sends to the dummy word
+// (0xFFFF - lo >= lim: lo + lim <= 2 * block entries < 0xFFFF).
 __device__ __forceinline__ void stream_tile(BatchSmem &sm, const BatchDyn &dd, const uint4 *__restrict__ ia4,
-                                            uint32_t ncv, void *scv, int ctile, bool wide, uint32_t lo, uint32_t lim,
-                                            int lane)
+                                            uint32_t ncv, void *scv, int ctile, bool wide, bool whole, uint32_t lo,
+                                            uint32_t lim, int lane)
 {
     const uint32_t M = dd.sp_pre[ncv];
     uint32_t *cnt = reinterpret_cast<uint32_t *>(scv);
     const uint32_t dummy = 2u * (uint32_t)ctile + (uint32_t)lane;   // packed: words [2T, 2T + 32)
+    const uint32_t fill = whole ? (dummy | (dummy << 16)) : 0xFFFFFFFFu;
     for (;;) {
         uint32_t u = 0;
         if (lane == 0) u = atomicAdd(&sm.next_unit, 1u);
@@ -521,34 +537,41 @@ __device__ __forceinline__ void stream_tile(BatchSmem &sm, const BatchDyn &dd, c
             if (j < M) {
                 while (dd.sp_pre[k + 1] <= j) k++;
                 kx[p] = k;
-                v[p] = __ldg(ia4 + (dd.sp_q0[k] + (j - dd.sp_pre[k])));
+                v[p] = __ldg(ia4 + (dd.sp_rec[k].x + j));
             }
         }
 #pragma unroll
         for (int p = 0; p < kChunks; p++) {
             if (kx[p] == 0xFFFFFFFFu) continue;
-            const uint32_t kk = kx[p];
+            const uint4 r = dd.sp_rec[kx[p]];
             const uint32_t j = j0 + (uint32_t)lane + 32u * p;
-            const uint32_t eq = (dd.sp_q0[kk] + (j - dd.sp_pre[kk])) << 3;
-            const uint32_t a0 = dd.sp_a0[kk], a1 = dd.sp_a1[kk];
-            const uint32_t c = dd.sp_c[kk], S = dd.sp_S[kk];
-            const uint32_t w4[4] = {v[p].x, v[p].y, v[p].z, v[p].w};
-            const bool full = eq >= a0 && eq + 8u <= a1;
+            const uint32_t eq = (r.x + j) << 3;   // element index of the chunk's first id
             if (!wide) {
-                const uint32_t vb = (c << 24) | S;
+                const uint32_t mlo = r.y > eq ? r.y - eq : 0u;      // 0..7
+                const uint32_t mhi = min(r.z - eq, 8u);             // 1..8
+                const uint4 kl = sm.keep_lo[mlo], kh = sm.keep_hi[mhi - 1u];
+                uint32_t w4[4] = {v[p].x, v[p].y, v[p].z, v[p].w};
+                const uint32_t km[4] = {kl.x & kh.x, kl.y & kh.y, kl.z & kh.z, kl.w & kh.w};
 #pragma unroll
-                for (int m = 0; m < 8; m++) {
-                    const uint32_t e = eq + (uint32_t)m;
-                    scatter_packed(cnt, (w4[m >> 1] >> (16 * (m & 1))) & 0xFFFFu, lo, lim, vb, dummy,
-                                   full || (e >= a0 && e < a1));
+                for (int q = 0; q < 4; q++) w4[q] = (w4[q] & km[q]) | (fill & ~km[q]);
+                if (whole) {
+#pragma unroll
+                    for (int m = 0; m < 8; m++) atomicAdd(cnt + ((w4[m >> 1] >> (16 * (m & 1))) & 0xFFFFu), r.w);
+                } else {
+#pragma unroll
+                    for (int m = 0; m < 8; m++)
+                        scatter_packed(cnt, (w4[m >> 1] >> (16 * (m & 1))) & 0xFFFFu, lo, lim, r.w, dummy, true);
                 }
             } else {
+                const uint32_t c = dd.sp_c[kx[p]];
+                const uint32_t w4[4] = {v[p].x, v[p].y, v[p].z, v[p].w};
+                const bool full = eq >= r.y && eq + 8u <= r.z;
 #pragma unroll
                 for (int m = 0; m < 8; m++) {
                     const uint32_t e = eq + (uint32_t)m;
-                    if (full || (e >= a0 && e < a1))
+                    if (full || (e >= r.y && e < r.z))
                         scatter_wide(cnt, cnt + ctile, cnt + 2 * ctile, (w4[m >> 1] >> (16 * (m & 1))) & 0xFFFFu, lo,
-                                     lim, c, S);
+                                     lim, c, r.w);
                 }
             }
         }
@@ -561,6 +584,17 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
     __shared__ BatchSmem sm;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     for (int i = tid; i < 81; i += kBBlock) sm.lgf[i] = a.lgfact[i];
+    if (tid < 16) {   // keep masks (table lo: ids >= m; table hi: ids < m + 1)
+        const int m = tid & 7;
+        uint32_t w[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const bool k0 = tid < 8 ? 2 * q >= m : 2 * q < m + 1;
+            const bool k1 = tid < 8 ? 2 * q + 1 >= m : 2 * q + 1 < m + 1;
+            w[q] = (k0 ? 0x0000FFFFu : 0u) | (k1 ? 0xFFFF0000u : 0u);
+        }
+        (tid < 8 ? sm.keep_lo : sm.keep_hi)[m] = make_uint4(w[0], w[1], w[2], w[3]);
+    }
     const int T = a.tile;
     void *scv = dyn;   // packed: T interleaved (b, y) word pairs; wide: 3 arrays of ctile words
     const BatchDyn dd = carve_dyn(dyn + (size_t)T * 8);
@@ -666,13 +700,16 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
                 const int tn = t1 - t0;
                 if (tn <= 0) continue;
                 const uint32_t lo = 2u * (uint32_t)(t0 - kb * E), lim = 2u * (uint32_t)tn;
+                // the tile is the whole block (all its entries): every id of the block is a word of it
+                const bool whole = !wide && (int64_t)t0 == kb * E && (int64_t)t1 == min((kb + 1) * E, (int64_t)ln.npep);
                 // ---- stream every interval's ids into the scorecard ----------------------
                 const bool prebuilt = sm.ready != 0u;   // built while the last tile was scored
                 for (uint32_t ic0 = 0; ic0 < nv; ic0 += kIvlChunk) {
                     const uint32_t ncv = min((uint32_t)kIvlChunk, nv - ic0);
                     if (!prebuilt) {
                         if (ti == 0 || nv > (uint32_t)kIvlChunk)
-                            build_span_table(sm, dd, ivl + ic0, ncv, bA, rel0, have, cur_s, cur_e, tid, lane, wid);
+                            build_span_table(sm, dd, ivl + ic0, ncv, bA, rel0, have, cur_s, cur_e, wide, tid, lane,
+                                             wid);
                         else if (tid == 0)
                             sm.next_unit = 0;
                         __syncthreads();
@@ -683,7 +720,7 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
                                             a.spill_per_warp, a.heap_cap, lane);
                         heap_due = false;
                     }
-                    stream_tile(sm, dd, ia4, ncv, scv, ctile, wide, lo, lim, lane);
+                    stream_tile(sm, dd, ia4, ncv, scv, ctile, wide, whole, lo, lim, lane);
                     if (ti == 0 && niA && tid < (int)nv) {   // the next tile's offsets, for its span table
                         dd.nx_s[tid] = nx_s;
                         dd.nx_e[tid] = nx_e;
