@@ -58,7 +58,9 @@ def make_workload(name: str, rank: int):
     w = WORKLOADS[name]
     t = time.time()
     db = gx.synth.make_database(w["nproteins"], seed=w["db_seed"])
+    t1 = time.perf_counter()
     H = gx.HostIndex.build(db, maxz=w["maxz"], mods=w["mods"], nmods=w["nmods"])
+    w = dict(w, host_build_s=time.perf_counter() - t1)
     q = gx.synth.make_queries(H.entries_by_len(), w["nspec"], seed=1000 + rank, **w["q"])
     log(f"[bench] workload {name}: {H.total_entries()} entries, {H.total_ions()} ion ids, {q.n} spectra, "
         f"{len(q.moz)} peaks ({time.time() - t:.1f}s)")
@@ -170,6 +172,7 @@ def main():
     ap.add_argument("--compare-plain", action="store_true", help="also time one step of the plain path")
     ap.add_argument("--spectra", type=int, default=0, help="search only the first N spectra (profiling cases)")
     ap.add_argument("--no-tail", action="store_true", help="leave the learned tail out of the step")
+    ap.add_argument("--no-index-build", action="store_true", help="skip timing the GPU index build at set-up")
     ap.add_argument("--sparse-below", type=int, default=500,
                     help="queries with fewer candidate PSMs take the learned tail")
     args = ap.parse_args()
@@ -215,7 +218,28 @@ def main():
         q = q.subset(np.arange(min(args.spectra, q.n)))
     params = gx.SearchParams(dM=w["dM"], dF=5, topmatches=5, expect_max=20.0,
                              flags=gx.FLAG_PLAIN if args.plain else 0)
+    t1 = time.perf_counter()
     dev = gx.DeviceIndex(H, local)
+    upload_s = time.perf_counter() - t1
+    # ---- index build: the same index with its fragment ions, CSR and block layout computed
+    # on the GPU (entries on the host), against the host build + upload above (untimed setup)
+    index_build = None
+    if not args.no_index_build:
+        t1 = time.perf_counter()
+        E = gx.HostIndex.build(db, maxz=w["maxz"], mods=w["mods"], nmods=w["nmods"], ions=False)
+        entries_s = time.perf_counter() - t1
+        t1 = time.perf_counter()
+        D = gx.DeviceIndex(E, local)
+        device_s = time.perf_counter() - t1
+        D.close()
+        E.close()
+        index_build = {"host_build_s": round(w["host_build_s"], 3), "upload_s": round(upload_s, 3),
+                       "entries_s": round(entries_s, 3), "device_ions_s": round(device_s, 3),
+                       "host_path_s": round(w["host_build_s"] + upload_s, 3),
+                       "device_path_s": round(entries_s + device_s, 3),
+                       "host_threads": os.cpu_count()}
+        log(f"[bench] index build: host {index_build['host_path_s']} s (build + upload), "
+            f"device {index_build['device_path_s']} s (entries + GPU ions/CSR)")
     ws = gx.Searcher(dev, q.n, len(q.moz))
     stream = torch.cuda.current_stream()
     d = torch.device("cuda", local)
@@ -393,6 +417,7 @@ def main():
             "kernel_ms": {k: v[1] / v[0] for k, v in kt.items()},
             "gpu_launches": launches,
             "path": "plain" if args.plain else ("batched+learned tail" if tail else "batched"),
+            "index_build": index_build,
             "learned_tail": dict(tail_info or {}, queries_replaced=int(
                 ((t_out.cpu().numpy().view(N.RESULT_DTYPE)["status"] & N.STATUS_LEARNED_TAIL) != 0).sum()))
             if tail else None,

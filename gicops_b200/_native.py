@@ -110,6 +110,11 @@ _SIGS = [
     ("gx_host_length_entries", C.c_void_p, [C.c_void_p]),
     ("gx_host_length_seqs", C.c_void_p, [C.c_void_p, C.POINTER(C.c_uint32)]),
     ("gx_host_length_free", None, [C.c_void_p]),
+    ("gx_build_length_entries", C.c_int32, [C.c_char_p, C.c_uint32, C.c_uint32, C.POINTER(BuildParams),
+                                            C.POINTER(C.c_void_p)]),
+    ("gx_index_build", C.c_int32, [C.POINTER(C.c_void_p), C.c_int32, C.POINTER(BuildParams), C.c_int32,
+                                   C.POINTER(C.c_void_p)]),
+    ("gx_index_read_length", C.c_int32, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("gx_workspace_create", C.c_int32, [C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(C.c_void_p)]),
     ("gx_workspace_free", C.c_int32, [C.c_void_p]),
     ("gx_search_host", C.c_int32, [C.c_void_p, C.c_void_p, C.POINTER(Queries), C.POINTER(Params), C.c_void_p,

@@ -27,57 +27,20 @@
 
 #include "../../include/gicops_b200.h"
 #include "gx_internal.h"
+#include "gx_ions.h"
 
 namespace {
 
-constexpr int kMaxSeqLen = 60;
-constexpr int kMaxModTypes = 15;
-
-// Residue masses and the fixed carbamidomethyl C (cmake/Templates/aamasses.hpp.in:25-80):
-// double literals narrowed to float, as the reference's constexpr float tables are.
-constexpr double kNAA = -20000.0;
-const float kAAMass[26] = {
-    (float)71.03712, (float)kNAA, (float)103.00919, (float)115.030, (float)129.0426, (float)147.068,
-    (float)57.02146, (float)137.060, (float)113.084, (float)kNAA, (float)128.094, (float)113.084,
-    (float)131.0405, (float)114.043, (float)kNAA, (float)97.0527, (float)128.05858, (float)156.1012,
-    (float)87.032, (float)101.0476, (float)kNAA, (float)99.06841, (float)186.0793, (float)kNAA,
-    (float)163.0633, (float)kNAA};
-const float kStatMod[26] = {0, 0, (float)57.021464, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0,
-                            0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-constexpr float kH2O = 18.015f;
-constexpr float kProton = 1.00727647f;
-
-inline int aa(char c) { return c - 'A'; }
-inline float aa_z(char c, unsigned z) { return (kAAMass[aa(c)] + kStatMod[aa(c)]) + (kProton * (float)z); }
-
-float pep_mass(const char *s, unsigned L)
-{
-    float m = kH2O;
-    for (unsigned l = 0; l < L; l++) m += kAAMass[aa(s[l])] + kStatMod[aa(s[l])];
-    return m;
-}
+using gx::ions::IonTables;
+using gx::ions::kMaxModTypes;
+using gx::ions::kMaxSeqLen;
 
 struct ModTable {
     int cond_of[256];            // residue -> modification type, -1 if none
     int limit;                   // modified residues per peptide
     std::vector<int> per_type;   // per-type limits
-    uint32_t mod_mass[kMaxModTypes];  // (uint)(mass*scale)
-    unsigned scale;
+    IonTables t;                 // residue tables, (uint)(mass*scale) per modification, scale
 };
-
-float mod_mass_first_only(const char *s, unsigned L, uint32_t modnum, const ModTable &mt)
-{
-    float m = kH2O;
-    for (unsigned l = 0; l < L; l++) {
-        m += kAAMass[aa(s[l])];
-        m += kStatMod[aa(s[l])];
-    }
-    // The reference's loop shifts by the mask (0xF0), which x86 reduces mod 32 to
-    // 16, so its second pass always reads 0: exactly one modification contributes.
-    const uint32_t first = modnum & 0x0Fu;
-    if (first != 0) m += ((float)mt.mod_mass[first - 1]) / (float)mt.scale;
-    return m;
-}
 
 void enumerate_variants(const char *seq, int L, std::vector<int> &left, int total, const gx_pep_entry &cont,
                         int letter, bool novel, int seen, uint32_t refid, const ModTable &mt,
@@ -85,7 +48,7 @@ void enumerate_variants(const char *seq, int L, std::vector<int> &left, int tota
 {
     if (novel && letter != 0) {
         gx_pep_entry e = cont;
-        e.mass = mod_mass_first_only(seq, (unsigned)L, e.modnum, mt);
+        e.mass = gx::ions::mod_mass_first_only(mt.t, seq, (unsigned)L, e.modnum);
         out.push_back(e);
     }
     if (total == 0 || letter >= L) return;
@@ -124,77 +87,6 @@ int cmp_variants(const void *l, const void *r)
     return 0;
 }
 
-// Theoretical spectrum (bins) of one entry into spec[speclen]; returns its mass.
-float entry_spectrum(const char *seq, unsigned L, const gx_pep_entry &e, unsigned maxz, double minmass,
-                     double maxmass, const ModTable &mt, std::vector<float> &f, uint32_t *spec, bool *filled)
-{
-    const unsigned scale = mt.scale;
-    const unsigned n1 = L - 1;
-    *filled = false;
-    float mass;
-    if (e.modnum == 0) {
-        mass = pep_mass(seq, L);
-        if (!(mass > 0)) return mass;
-    } else {
-        if (e.sites == 0) return (float)kNAA;
-        mass = mod_mass_first_only(seq, L, e.modnum, mt);
-        if (!(mass > minmass && mass < maxmass)) return mass;
-    }
-    f.assign((size_t)2 * maxz * n1, 0.0f);
-    for (unsigned z = 0; z < maxz; z++) {
-        const unsigned bs = z * n1, ys = z * n1 + maxz * n1;
-        f[bs] = aa_z(seq[0], z + 1);
-        f[ys] = aa_z(seq[L - 1], z + 1) + kH2O;
-        for (unsigned l = 1; l < n1; l++) {
-            f[bs + l] = f[bs + l - 1] + aa_z(seq[l], 0);
-            f[ys + l] = f[ys + l - 1] + aa_z(seq[L - 1 - l], 0);
-        }
-    }
-    if (e.modnum == 0) {
-        for (unsigned z = 0; z < maxz; z++) {
-            const unsigned bs = z * n1, ys = z * n1 + maxz * n1;
-            for (unsigned l = 0; l < n1; l++) {
-                spec[bs + l] = (uint32_t)((f[bs + l] * (float)scale) / (float)(z + 1));
-                spec[ys + l] = (uint32_t)((f[ys + l] * (float)scale) / (float)(z + 1));
-            }
-        }
-    } else {
-        int nums[kMaxModTypes];
-        int seen = 0;
-        uint32_t mask = e.modnum;
-        for (int i = 0; i < kMaxModTypes; i++) {
-            nums[i] = (int)(mask & 0x0Fu) - 1;
-            mask /= 16;
-            if (nums[i] != -1) seen++;
-        }
-        char pos[kMaxSeqLen + 2];
-        for (unsigned i = 0; i < L; i++) pos[i] = ((e.sites >> i) & 1u) ? 1 : 0;
-        for (unsigned z = 0; z < maxz; z++) {
-            const unsigned bs = z * n1;
-            unsigned cnt = 0;
-            for (unsigned l = 0; l < n1; l++) {
-                cnt += (unsigned)pos[l];
-                for (unsigned k = 0; k < cnt; k++)
-                    f[bs + l] = (float)((double)f[bs + l] + (double)mt.mod_mass[nums[k]] / (double)scale);
-                spec[bs + l] = (uint32_t)(f[bs + l] * (float)scale / (float)(z + 1));
-            }
-        }
-        for (unsigned z = 0; z < maxz; z++) {
-            const unsigned ys = z * n1 + maxz * n1;
-            unsigned cnt = 0;
-            for (int l = (int)n1; l > 0; l--) {
-                cnt += (unsigned)pos[l];
-                const unsigned o = ys + n1 - (unsigned)l;
-                for (unsigned k = 0; k < cnt; k++)
-                    f[o] = (float)((double)f[o] + (double)mt.mod_mass[nums[seen - 1 - (int)k]] / (double)scale);
-                spec[o] = (uint32_t)(f[o] * (float)scale / (float)(z + 1));
-            }
-        }
-    }
-    *filled = true;
-    return mass;
-}
-
 }  // namespace
 
 struct gx_host_length {
@@ -205,8 +97,11 @@ struct gx_host_length {
     std::vector<uint32_t> bA, iA;
 };
 
-extern "C" gx_status gx_build_length(const char *seqs, uint32_t npep, uint32_t L, const gx_build_params *bp,
-                                     gx_host_length **out)
+namespace {
+
+// Steps 1-2 of a build: mass filter, variant enumeration, mass sort (into h).
+gx_status build_entries(const char *seqs, uint32_t npep, uint32_t L, const gx_build_params *bp, gx_host_length **out,
+                        ModTable &mt)
 {
     using namespace gx;
     if (!out || !bp || (!seqs && npep)) return fail(GX_ERR_INVLD_PTR, "gx_build_length: null argument");
@@ -216,16 +111,13 @@ extern "C" gx_status gx_build_length(const char *seqs, uint32_t npep, uint32_t L
         return fail(GX_ERR_INVLD_PARAM, "gx_build_length: bad parameters");
     const int threads = bp->threads > 0 ? bp->threads : omp_get_max_threads();
 
-    ModTable mt;
     for (int &c : mt.cond_of) c = -1;
     mt.limit = (int)bp->mods_per_pep;
-    mt.scale = bp->scale;
-    std::memset(mt.mod_mass, 0, sizeof(mt.mod_mass));
+    mt.t = gx::ion_tables(bp);
     for (uint32_t i = 0; i < bp->nmods; i++) {
         for (int j = 0; j < 4 && bp->mods[i].residues[j]; j++)
             mt.cond_of[(unsigned char)bp->mods[i].residues[j]] = (int)i;
         mt.per_type.push_back((int)bp->mods[i].max_per_pep);
-        mt.mod_mass[i] = (uint32_t)(bp->mods[i].mass * (double)bp->scale);
     }
     for (uint64_t i = 0; i < (uint64_t)npep * L; i++)
         if (seqs[i] < 'A' || seqs[i] > 'Z') return fail(GX_ERR_INVLD_PARAM, "gx_build_length: non-letter residue");
@@ -241,7 +133,7 @@ extern "C" gx_status gx_build_length(const char *seqs, uint32_t npep, uint32_t L
     std::vector<uint32_t> kept;
     std::vector<float> kmass;
     for (uint32_t i = 0; i < npep; i++) {
-        const float m = pep_mass(seqs + (size_t)i * L, L);
+        const float m = gx::ions::pep_mass(mt.t, seqs + (size_t)i * L, L);
         if (m >= (float)bp->min_mass && m <= (float)bp->max_mass) {
             kept.push_back(i);
             kmass.push_back(m);
@@ -282,6 +174,28 @@ extern "C" gx_status gx_build_length(const char *seqs, uint32_t npep, uint32_t L
               [](const gx_pep_entry &a, const gx_pep_entry &b) { return a.mass < b.mass; });
     h->mass.resize(N);
     for (uint64_t k = 0; k < N; k++) h->mass[k] = h->entries[k].mass;
+    *out = h;
+    return GX_SUCCESS;
+}
+
+}  // namespace
+
+extern "C" gx_status gx_build_length_entries(const char *seqs, uint32_t npep, uint32_t L, const gx_build_params *bp,
+                                             gx_host_length **out)
+{
+    ModTable mt;
+    return build_entries(seqs, npep, L, bp, out, mt);
+}
+
+extern "C" gx_status gx_build_length(const char *seqs, uint32_t npep, uint32_t L, const gx_build_params *bp,
+                                     gx_host_length **out)
+{
+    ModTable mt;
+    gx_host_length *h = nullptr;
+    const gx_status st = build_entries(seqs, npep, L, bp, &h, mt);
+    if (st != GX_SUCCESS) return st;
+    const int threads = bp->threads > 0 ? bp->threads : omp_get_max_threads();
+    const uint64_t N = h->entries.size();
 
     // 3. fragment ions -> bins; 4. stable counting sort by bin
     const uint32_t speclen = h->speclen;
@@ -293,22 +207,19 @@ extern "C" gx_status gx_build_length(const char *seqs, uint32_t npep, uint32_t L
     {
         const int t = omp_get_thread_num();
         const uint64_t k0 = N * t / T, k1 = N * (t + 1) / T;
-        std::vector<float> f;
-        std::vector<uint32_t> spec(speclen);
         uint32_t *c = cnt[t].data();
+        const uint32_t n1 = L - 1;
         for (uint64_t k = k0; k < k1; k++) {
             const gx_pep_entry &e = h->entries[k];
-            bool filled = false;
-            const float m = entry_spectrum(&h->seqs[(size_t)e.seqid * L], L, e, bp->maxz, (double)bp->min_mass,
-                                           (double)bp->max_mass, mt, f, spec.data(), &filled);
+            const char *seq = &h->seqs[(size_t)e.seqid * L];
             uint32_t *dst = &bins[(size_t)k * speclen];
-            if (filled && m >= (double)bp->min_mass && m <= (double)bp->max_mass) {
-                for (uint32_t ion = 0; ion < speclen; ion++) {
-                    uint32_t b = spec[ion];
-                    if ((double)b >= (double)topbin) b = topbin - 1;
-                    dst[ion] = b;
-                    c[b]++;
+            if (gx::ions::entry_binned(mt.t, seq, L, e.sites, e.modnum, (double)bp->min_mass, (double)bp->max_mass)) {
+                // positions: b ions of charge z at z*(L-1), y ions at (maxz + z)*(L-1)
+                for (uint32_t z = 0; z < bp->maxz; z++) {
+                    gx::ions::ion_series(mt.t, seq, L, e.sites, e.modnum, z, false, topbin, dst + z * n1);
+                    gx::ions::ion_series(mt.t, seq, L, e.sites, e.modnum, z, true, topbin, dst + (bp->maxz + z) * n1);
                 }
+                for (uint32_t ion = 0; ion < speclen; ion++) c[dst[ion]]++;
             } else {
                 std::memset(dst, 0, sizeof(uint32_t) * speclen);
                 c[0] += speclen;
@@ -350,8 +261,8 @@ extern "C" gx_status gx_host_length_desc(const gx_host_length *h, gx_length_desc
     d->speclen = h->speclen;
     d->pad = 0;
     d->mass = h->mass.data();
-    d->bA = h->bA.data();
-    d->iA = h->iA.data();
+    d->bA = h->bA.empty() ? nullptr : h->bA.data();   // entries-only lengths have no CSR
+    d->iA = h->iA.empty() ? nullptr : h->iA.data();
     return GX_SUCCESS;
 }
 

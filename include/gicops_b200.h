@@ -110,6 +110,25 @@ gx_status gx_host_length_desc(const gx_host_length *h, gx_length_desc *desc);
 const gx_pep_entry *gx_host_length_entries(const gx_host_length *h);
 const char *gx_host_length_seqs(const gx_host_length *h, uint32_t *npep_kept);
 void gx_host_length_free(gx_host_length *h);
+/* Entries of one length only (mass filter, variant enumeration, mass sort: the steps
+ * of gx_build_length before the fragment ions), for gx_index_build, which computes the
+ * ions on the GPU.  The descriptor of such a length has bA = iA = NULL. */
+gx_status gx_build_length_entries(const char *seqs, uint32_t npep, uint32_t L, const gx_build_params *bp,
+                                  gx_host_length **out);
+
+/* ---- device index builder (DSLIM_Construct's ion and CSR stage, dslim.cpp:231-504 with
+ * the ion arithmetic of utils.cpp:161-474, on the GPU, plus s1::getdIndex) ------------
+ * Builds the device-resident index on `device` from host lengths (gx_build_length or
+ * gx_build_length_entries with the same gx_build_params, in idxoffset order): fragment
+ * ions, bA / iA and the block layout are computed on the GPU and equal those of
+ * gx_index_upload of the host-built lengths.  At most 2^31 - 1 ion ids per length. */
+gx_status gx_index_build(gx_host_length *const *lens, int32_t nlen, const gx_build_params *bp, int32_t device,
+                         gx_index **out);
+/* Copy one length of a device index to the host (any pointer may be NULL): bA [nbins],
+ * iA [npep*speclen] with ids as the device holds them (2*entry + (y ion)), iAb
+ * [npep*speclen] (block-local 16-bit ids), mass [npep].  No counterpart in the reference. */
+gx_status gx_index_read_length(const gx_index *ix, int32_t i, uint32_t *bA, uint32_t *iA, uint16_t *iAb,
+                               float *mass);
 
 /* ---- search ------------------------------------------------------------------------ */
 typedef struct {

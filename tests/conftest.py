@@ -34,15 +34,16 @@ def case_queries(c: dict):
                       np.zeros(len(c["q_prec"]), np.float32), dM)
 
 
-def case_index(c: dict):
-    """Index of a golden case built by the library's host builder."""
+def case_index(c: dict, ions: bool = True):
+    """Index of a golden case built by the library's host builder (entries only when
+    ions is False)."""
     import gicops_b200 as gx
     from gicops_b200.synth import Database
     m = c["meta"]
     db = Database(peps=c["peps"], nproteins=m["nproteins"])
     mods = [tuple(x) for x in m["mods"]]
     return gx.HostIndex.build(db, maxz=m["maxz"], mods=mods, nmods=m["nmods"], min_mass=m["min_mass"],
-                              max_mass=m["max_mass"])
+                              max_mass=m["max_mass"], ions=ions)
 
 
 def oracle_params(c: dict):

@@ -59,3 +59,36 @@ def test_builder_rejects_bad_input():
     seq = np.frombuffer(b"PEPTIDE", np.uint8).copy()
     assert L.gx_build_length(seq.ctypes.data_as(C.c_char_p), 1, 7, C.byref(bp0), C.byref(h)) == -3002
     assert L.gx_build_length(seq.ctypes.data_as(C.c_char_p), 1, 7, None, C.byref(h)) == -3008
+
+
+def test_entries_only_build_matches_full_build():
+    """ions=False stops after the entries: same entries, masses and sequences, no CSR."""
+    import gicops_b200 as gx
+    db = gx.synth.make_database(120, seed=5)
+    a = gx.HostIndex.build(db, maxz=2, mods=[("M", 15.9949, 2)], nmods=2)
+    b = gx.HostIndex.build(db, maxz=2, mods=[("M", 15.9949, 2)], nmods=2, ions=False)
+    assert [x["L"] for x in a.lengths] == [x["L"] for x in b.lengths]
+    for x, y in zip(a.lengths, b.lengths):
+        assert x["N"] == y["N"] and x["speclen"] == y["speclen"]
+        assert x["entries"].tobytes() == y["entries"].tobytes()
+        assert x["mass"].tobytes() == y["mass"].tobytes()
+        assert x["seqs"].tobytes() == y["seqs"].tobytes()
+        assert y["bA"] is None and y["iA"] is None
+    with pytest.raises(ValueError):
+        gx.DeviceIndex(b, 0, on_device=False)   # no CSR to upload (raised before any device call)
+
+
+def test_device_build_rejects_mismatched_lengths():
+    """gx_index_build checks its lengths on the host before any device call."""
+    import gicops_b200 as gx
+    import ctypes as C
+    import gicops_b200._native as N
+    from gicops_b200.index import _build_params
+    db = gx.synth.make_database(50, seed=3)
+    H = gx.HostIndex.build(db, maxz=2, ions=False)
+    bp, marr = _build_params(1, (), 0, 500, 5000, 100, 0)       # maxz 1 vs lengths built at 2
+    hs = (C.c_void_p * H.nlen)(*[x["handle"] for x in H.lengths])
+    out = C.c_void_p()
+    assert N.lib().gx_index_build(hs, H.nlen, C.byref(bp), 0, C.byref(out)) == -3003 and not out
+    bp2, marr2 = _build_params(2, (), 0, 500, 5000, 100, 0)
+    assert N.lib().gx_index_build(hs, 0, C.byref(bp2), 0, C.byref(out)) == -3002 and not out
