@@ -6,7 +6,7 @@ of include/gicops_b200.h.  A drop-in for the reference's (mhaseeb123/gicops)
 ``hcp::gpu::cuda::s3::search`` / ``DSLIM_QuerySpectrum`` boundary.
 """
 
-from . import synth, tail
+from . import prep, synth, tail
 from ._native import (CELL_DTYPE, FLAG_PLAIN, FLAG_WIDE_SCORECARD, HIST_BINS, PEP_ENTRY_DTYPE, RESULT_DTYPE,
                       GxError, lib)
 from .index import DeviceIndex, HostIndex

@@ -71,6 +71,12 @@ class LengthDesc(C.Structure):
                 ("mass", C.c_void_p), ("bA", C.c_void_p), ("iA", C.c_void_p)]
 
 
+class Ms2Raw(C.Structure):
+    _fields_ = [("nspec", C.c_uint32), ("nvalues", C.c_uint32), ("seg", C.c_void_p), ("size", C.c_void_p),
+                ("mz", C.c_void_p), ("intn", C.c_void_p), ("prec", C.c_void_p), ("charge", C.c_void_p),
+                ("rtime", C.c_void_p)]
+
+
 class Mod(C.Structure):
     _fields_ = [("residues", C.c_char * 4), ("mass", C.c_double), ("max_per_pep", C.c_uint32)]
 
@@ -115,6 +121,11 @@ _SIGS = [
     ("gx_index_build", C.c_int32, [C.POINTER(C.c_void_p), C.c_int32, C.POINTER(BuildParams), C.c_int32,
                                    C.POINTER(C.c_void_p)]),
     ("gx_index_read_length", C.c_int32, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("gx_ms2_read", C.c_int32, [C.c_char_p, C.c_uint32, C.POINTER(C.c_void_p)]),
+    ("gx_ms2_desc", C.c_int32, [C.c_void_p, C.POINTER(Ms2Raw)]),
+    ("gx_ms2_free", None, [C.c_void_p]),
+    ("gx_pickpeaks_device", C.c_int32, [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
+                                        C.c_int32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("gx_workspace_create", C.c_int32, [C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(C.c_void_p)]),
     ("gx_workspace_free", C.c_int32, [C.c_void_p]),
     ("gx_search_host", C.c_int32, [C.c_void_p, C.c_void_p, C.POINTER(Queries), C.POINTER(Params), C.c_void_p,

@@ -102,6 +102,7 @@ extern "C" gx_status gx_index_free(gx_index *ix)
     cudaFree(ix->mass);
     cudaFree(ix->lens);
     delete ix;
+    cudaGetLastError();   // nothing of a free is reported to the next call
     return GX_SUCCESS;
 }
 
@@ -209,6 +210,7 @@ extern "C" gx_status gx_index_upload(const gx_length_desc *lens, int32_t nlen, u
     *out = nullptr;
     if (nlen < 1 || nlen > GX_MAX_LENGTHS || nbins < 2)
         return fail(GX_ERR_INVLD_PARAM, "gx_index_upload: nlen must be 1..64 and nbins >= 2");
+    cudaGetLastError();   // an earlier call's error is not ours to report
     uint32_t maxz = 0;
     uint64_t tot_ia = 0, tot_m = 0, tot_blk = 0;
     std::vector<DevLen> hl(nlen);
@@ -237,24 +239,28 @@ extern "C" gx_status gx_index_upload(const gx_length_desc *lens, int32_t nlen, u
                                "gx_index_upload");
     if (st != GX_SUCCESS) return st;
     cudaError_t e = cudaSuccess;
+    const char *step = "";
     for (int i = 0; i < nlen && e == cudaSuccess; i++) {
         const gx_length_desc &d = lens[i];
+        step = "gx_index_upload: bA copy";
         if ((e = cudaMemcpy(ix->bA + (uint64_t)i * nbins, d.bA, sizeof(uint32_t) * nbins, cudaMemcpyHostToDevice)) !=
             cudaSuccess)
             break;
         if (!d.npep) continue;
         const uint64_t nid = (uint64_t)d.npep * d.speclen;
+        step = "gx_index_upload: iA / mass copy";
         if ((e = cudaMemcpy(ix->iA + hl[i].ia_off, d.iA, sizeof(uint32_t) * nid, cudaMemcpyHostToDevice)) !=
                 cudaSuccess ||
             (e = cudaMemcpy(ix->mass + hl[i].mass_off, d.mass, sizeof(float) * d.npep, cudaMemcpyHostToDevice)) !=
                 cudaSuccess)
             break;
+        step = "gx_index_upload: id encoding / block layout";
         e = finish_length(ix, i, scan_tmp, scan_bytes);
     }
     cudaFree(scan_tmp);
     if (e != cudaSuccess) {
         gx_index_free(ix);
-        return cuda_fail(e, "gx_index_upload");
+        return cuda_fail(e, step);
     }
     if ((st = finish_index(ix, "gx_index_upload")) != GX_SUCCESS) return st;
     *out = ix;
@@ -322,6 +328,7 @@ extern "C" gx_status gx_index_build(gx_host_length *const *lens, int32_t nlen, c
     if (!lens || !bp || !out) return fail(GX_ERR_INVLD_PTR, "gx_index_build: null argument");
     *out = nullptr;
     if (nlen < 1 || nlen > GX_MAX_LENGTHS) return fail(GX_ERR_INVLD_PARAM, "gx_index_build: nlen must be 1..64");
+    cudaGetLastError();   // an earlier call's error is not ours to report
     if (bp->maxz < 1 || bp->maxz > 6 || bp->scale == 0 || bp->max_mass <= bp->min_mass ||
         bp->nmods > (uint32_t)ions::kMaxModTypes)
         return fail(GX_ERR_INVLD_PARAM, "gx_index_build: bad parameters");
@@ -383,6 +390,7 @@ extern "C" gx_status gx_index_build(gx_host_length *const *lens, int32_t nlen, c
         (e = cudaMalloc(&d_ent, sizeof(gx_pep_entry) * std::max<uint64_t>(max_ent, 1))) != cudaSuccess)
         cudaGetLastError();
     const ions::IonTables tab = ion_tables(bp);
+    const char *step = "gx_index_build: build scratch";
     const int end_bit = 32 - __builtin_clz(topbin);
     for (int i = 0; i < nlen && e == cudaSuccess; i++) {
         const Src &x = src[i];
@@ -393,9 +401,11 @@ extern "C" gx_status gx_index_build(gx_host_length *const *lens, int32_t nlen, c
             continue;
         }
         const uint64_t n = (uint64_t)N * x.d.speclen;
+        step = "gx_index_build: entry copy";
         if ((e = cudaMemcpy(d_seqs, x.seqs, (size_t)x.nkept * L, cudaMemcpyHostToDevice)) != cudaSuccess ||
             (e = cudaMemcpy(d_ent, x.ent, sizeof(gx_pep_entry) * N, cudaMemcpyHostToDevice)) != cudaSuccess)
             break;
+        step = "gx_index_build: ions / sort / offsets";
         const uint64_t threads = (uint64_t)N * 2 * bp->maxz;
         k_ions<<<(unsigned)std::min<uint64_t>((threads + 255) / 256, 1u << 20), 256>>>(
             d_seqs, d_ent, N, L, bp->maxz, tab, (double)bp->min_mass, (double)bp->max_mass, topbin, keys, vals);
@@ -411,6 +421,7 @@ extern "C" gx_status gx_index_build(gx_host_length *const *lens, int32_t nlen, c
         k_entry_mass<<<(N + 255) / 256, 256>>>(d_ent, N, ix->mass + hl[i].mass_off);
         count_launch();
         if ((e = cudaGetLastError()) != cudaSuccess) break;
+        step = "gx_index_build: id encoding / block layout";
         e = finish_length(ix, i, scan_tmp, scan_bytes);
     }
     cudaDeviceSynchronize();
@@ -424,7 +435,7 @@ extern "C" gx_status gx_index_build(gx_host_length *const *lens, int32_t nlen, c
     if (e != cudaSuccess) {
         gx_index_free(ix);
         if (e == cudaErrorMemoryAllocation) return fail(GX_ERR_BAD_MEM_ALLOC, "gx_index_build: build scratch");
-        return cuda_fail(e, "gx_index_build");
+        return cuda_fail(e, step);
     }
     if ((st = finish_index(ix, "gx_index_build")) != GX_SUCCESS) return st;
     *out = ix;

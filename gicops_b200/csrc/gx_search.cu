@@ -371,6 +371,7 @@ constexpr int kDefaultTile = 8192;   // plain path: candidates per scorecard til
 
 struct gx_workspace {
     const gx_index *ix = nullptr;
+    int device = 0;   // the index's device (the index may be freed first)
     uint32_t max_spec = 0, max_peaks = 0;
     int2 *win = nullptr;
     double *lgfact = nullptr;
@@ -453,13 +454,14 @@ extern "C" int32_t gx_heap_capacity(uint32_t topmatches)
 extern "C" gx_status gx_workspace_free(gx_workspace *ws)
 {
     if (!ws) return GX_SUCCESS;
-    if (ws->ix) cudaSetDevice(ws->ix->device);
+    cudaSetDevice(ws->device);
     void *ptrs[] = {ws->win, ws->lgfact, ws->err, ws->qidx, ws->moz, ws->intn, ws->charge, ws->prec,
                     ws->dMq, ws->out, ws->heap, ws->hist, ws->ivl, ws->nivl, ws->guard, ws->queue,
                     ws->hist_g, ws->spill, ws->logtab, ws->bs.key_in, ws->bs.key_out, ws->bs.ord_in, ws->bs.ord_out, ws->bs.sort_temp};
     for (void *p : ptrs) cudaFree(p);
     if (ws->stream) cudaStreamDestroy(ws->stream);
     delete ws;
+    cudaGetLastError();   // nothing of a free is reported to the next call
     return GX_SUCCESS;
 }
 
@@ -472,6 +474,7 @@ extern "C" gx_status gx_workspace_create(const gx_index *ix, uint32_t max_spec, 
     GX_CUDA(cudaSetDevice(ix->device));
     auto *ws = new gx_workspace();
     ws->ix = ix;
+    ws->device = ix->device;
     ws->max_spec = max_spec;
     ws->max_peaks = max_peaks;
     cudaError_t e = cudaSuccess;

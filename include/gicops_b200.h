@@ -33,6 +33,7 @@ typedef int32_t gx_status;
 #define GX_ERR_INVLD_PARAM     (-3002)
 #define GX_ERR_INVLD_INDEX     (-3003)
 #define GX_ERR_INVLD_SIZE      (-3004)
+#define GX_ERR_FILE_NOT_FOUND  (-3006)
 #define GX_ERR_BAD_MEM_ALLOC   (-3007)
 #define GX_ERR_INVLD_PTR       (-3008)
 #define GX_ERR_INVLD_MOD       (-3010)
@@ -129,6 +130,43 @@ gx_status gx_index_build(gx_host_length *const *lens, int32_t nlen, const gx_bui
  * [npep*speclen] (block-local 16-bit ids), mass [npep].  No counterpart in the reference. */
 gx_status gx_index_read_length(const gx_index *ix, int32_t i, uint32_t *bA, uint32_t *iA, uint16_t *iAb,
                                float *mass);
+
+/* ---- query preprocessing (MSQuery::convertAndprepMS2bin, msquery.cpp:137-336) -------- */
+typedef struct gx_ms2_file gx_ms2_file;   /* raw spectra read from an MS2 file (opaque) */
+
+/* Raw spectra as the reference collects them before peak picking.  Spectrum s owns the
+ * values [seg[s], seg[s+1]) (normally size[s] of them; values before a file's first S
+ * line belong to the first spectrum, whose size counts only the lines after its S). */
+typedef struct {
+    uint32_t nspec, nvalues;
+    const uint32_t *seg;     /* [nspec + 1] */
+    const uint32_t *size;    /* [nspec] */
+    const int32_t *mz;       /* [nvalues] (int)(m/z * scale) */
+    const int32_t *intn;     /* [nvalues] (int)(intensity * 100) */
+    const float *prec;       /* [nspec] precursor M+H from the Z line */
+    const int32_t *charge;   /* [nspec] */
+    const float *rtime;      /* [nspec] */
+} gx_ms2_raw;
+
+/* Read an MS2 text file with the reference's parsing rules (the first half of
+ * convertAndprepMS2bin); scale = bins per Da (100). */
+gx_status gx_ms2_read(const char *path, uint32_t scale, gx_ms2_file **out);
+gx_status gx_ms2_desc(const gx_ms2_file *f, gx_ms2_raw *raw);
+void gx_ms2_free(gx_ms2_file *f);
+
+/* Peak picking and intensity normalisation on the GPU (MSQuery::pickpeaks,
+ * msquery.cpp:338-423, with the key-value quicksort of include/keyval.h:49-129): per
+ * spectrum the first size[s] values of its segment are sorted by intensity (the
+ * reference's exact quicksort, so ties keep its order), the top one is set to base_int
+ * and the others scaled by base_int / top (truncated to int), and the peaks from the
+ * top down to the first one below min_int, at most qalen, are kept: the last `kept`
+ * values of the segment, in ascending intensity.  Device arrays, stream-ordered;
+ * mz_dev / intn_dev are sorted and scaled in place; out_idx_dev [nspec + 1] receives the
+ * kept peaks' CSR offsets and out_mz_dev / out_intn_dev (capacity nvalues) the peaks.
+ * The reference's defaults: base_int 100000, min_int 1000, qalen 100. */
+gx_status gx_pickpeaks_device(uint32_t nspec, const uint32_t *seg_dev, const uint32_t *size_dev, int32_t *mz_dev,
+                              int32_t *intn_dev, int32_t base_int, int32_t min_int, uint32_t qalen,
+                              uint32_t *out_idx_dev, int32_t *out_mz_dev, int32_t *out_intn_dev, void *stream);
 
 /* ---- search ------------------------------------------------------------------------ */
 typedef struct {

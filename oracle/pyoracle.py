@@ -162,3 +162,26 @@ def traffic(lengths, q, params: Params):
                      C.c_float(q.prec[i]), C.c_double(dm), C.byref(par), C.byref(a), C.byref(b))
         ids[i], bins[i] = a.value, b.value
     return ids, bins
+
+
+def pickpeaks(seg, size, mz, intn, base_int=100000, min_int=1000, qalen=100):
+    """Peak picking of raw spectra (rs_pickpeaks per spectrum, on copies of mz/intn):
+    returns (idx[n+1], mz, intn) of the kept peaks."""
+    L = lib()
+    L.rs_pickpeaks.restype = C.c_int
+    mz = np.ascontiguousarray(mz, dtype=np.int32).copy()
+    intn = np.ascontiguousarray(intn, dtype=np.int32).copy()
+    n = len(size)
+    idx = np.zeros(n + 1, np.uint32)
+    out_m, out_i = [], []
+    for s in range(n):
+        a, b = int(seg[s]), int(seg[s + 1])
+        S = min(int(size[s]), b - a)
+        m, i = mz[a:b], intn[a:b]                       # views: sorted and scaled in place
+        k = L.rs_pickpeaks(m.ctypes.data_as(C.c_void_p), i.ctypes.data_as(C.c_void_p), C.c_int(b - a), C.c_int(S),
+                           C.c_int32(base_int), C.c_int32(min_int), C.c_int(qalen))
+        out_m.append(m[b - a - k:].copy())
+        out_i.append(i[b - a - k:].copy())
+        idx[s + 1] = idx[s] + k
+    cat = lambda xs: np.concatenate(xs).astype(np.int32) if xs else np.zeros(0, np.int32)
+    return idx, cat(out_m), cat(out_i)

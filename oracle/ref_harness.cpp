@@ -19,6 +19,7 @@
 //               [--expect-max 1e300] [--queries Q.pbin] [--first N] [--repeat R]
 //               [--out RES.bin] [--dump-index IDX.bin] [--qdm DM.f64]
 //               [--min-cpsm 4] [--min-shp 4]
+//   ref_harness --ms2-to-pbin FILE.ms2     (the reference's MS2 conversion: FILE.ms2.pbin)
 // --qdm gives one precursor tolerance (Da, float64) per spectrum: each spectrum is then
 // searched alone with params.dM set to its value (the reference reads params.dM at
 // call time in DSLIM_BinarySearch, source/core/dslim_query.cpp:1102-1106).
@@ -37,6 +38,7 @@
 #include "config.hpp"
 #include "dslim.h"
 #include "dslim_fileout.h"
+#include "msquery.hpp"
 #include "expeRT.h"
 #include "lbe.h"
 #include "mods.h"
@@ -124,9 +126,15 @@ static bool read_pbin(const std::string &path, std::vector<Spec> &out)
     return true;
 }
 
+// The reference's MS2 -> .pbin converter (source/core/msquery.cpp:137-336: parsing, peak
+// picking and intensity normalisation of msquery.cpp:338-423) is a protected static member.
+struct Ms2Converter : MSQuery {
+    static std::array<int, 2> run(std::string *path) { return convertAndprepMS2bin(path); }
+};
+
 int main(int argc, char **argv)
 {
-    std::string db, qpath, outpath, dumppath, qdmpath;
+    std::string db, qpath, outpath, dumppath, qdmpath, ms2path;
     std::vector<std::string> mods;
     int minlen = 6, maxlen = 46, maxz = 1, nmods = 0, threads = omp_get_max_threads();
     int topmatches = 5, first = -1, repeat = 1, min_cpsm = 4, min_shp = 4;
@@ -158,7 +166,17 @@ int main(int argc, char **argv)
         else if (a == "--qdm") qdmpath = nxt();
         else if (a == "--min-cpsm") min_cpsm = std::atoi(nxt().c_str());
         else if (a == "--min-shp") min_shp = std::atoi(nxt().c_str());
+        else if (a == "--ms2-to-pbin") ms2path = nxt();
         else { std::fprintf(stderr, "unknown option %s\n", a.c_str()); return 2; }
+    }
+    if (!ms2path.empty()) {
+        // writes <ms2path>.pbin with the reference's default scale and intensity parameters
+        params.scale = 100;
+        params.base_int = 1000 * YAXISMULTIPLIER;
+        params.min_int = (int)(params.base_int * 0.01 + 0.5);
+        const std::array<int, 2> r = Ms2Converter::run(&ms2path);
+        std::printf("{\"spectra\": %d, \"largest\": %d}\n", r[0], r[1]);
+        return 0;
     }
     if (db.empty()) { std::fprintf(stderr, "--db is required\n"); return 2; }
 

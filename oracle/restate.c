@@ -431,3 +431,59 @@ void rs_traffic(const rs_length *lens, int nlen, const int32_t *moz, int npk, fl
     *ids = ni;
     *bins = nb;
 }
+
+/* ---- query preprocessing: peak picking and intensity normalisation -------------------
+ * source/core/msquery.cpp:338-423 (MSQuery::pickpeaks, the form the MS2 -> .pbin
+ * conversion uses) with the key-value quicksort of source/core/include/keyval.h:49-129
+ * (Hoare partition around the middle element; its OpenMP tasks only split disjoint
+ * ranges, so the result is that of the serial recursion). */
+
+/* double -> int32 as x86's truncating conversion does it: out-of-range and NaN give
+ * INT32_MIN (the reference converts with an implicit int cast). */
+int32_t rs_cvt_i32(double v)
+{
+    return (v >= -2147483648.0 && v < 2147483648.0) ? (int32_t)v : INT32_MIN;
+}
+
+static void kv_sort(int32_t *key, int32_t *val, long left, long right)
+{
+    long i = left, j = right;
+    const int32_t pivot = key[(left + right) / 2];
+    while (i <= j) {
+        while (key[i] < pivot) i++;
+        while (key[j] > pivot) j--;
+        if (i <= j) {
+            const int32_t tk = key[i], tv = val[i];
+            key[i] = key[j];
+            val[i] = val[j];
+            key[j] = tk;
+            val[j] = tv;
+            i++;
+            j--;
+        }
+    }
+    if (left < j) kv_sort(key, val, left, j);
+    if (i < right) kv_sort(key, val, i, right);
+}
+
+/* One spectrum: mz/in hold the n_vec values collected since the previous spectrum
+ * (n_vec == specsize except for peaks before a file's first S line); the first specsize
+ * are sorted by intensity and scaled in place.  Returns the number of peaks kept: the
+ * last `kept` values of the arrays. */
+int rs_pickpeaks(int32_t *mz, int32_t *in, int n_vec, int specsize, int32_t base_int, int32_t min_int, int qalen)
+{
+    (void)n_vec;
+    if (specsize <= 0) return 0;
+    kv_sort(in, mz, 0, specsize - 1);
+    const double factor = (double)base_int / (double)in[specsize - 1];
+    in[specsize - 1] = base_int;
+    int kept = 1;
+    for (int j = specsize - 2; j >= specsize - qalen && j >= 0; j--) {
+        in[j] = rs_cvt_i32((double)in[j] * factor);
+        if (in[j] >= min_int)
+            kept++;
+        else
+            break;
+    }
+    return kept >= qalen ? qalen : kept;
+}

@@ -96,7 +96,12 @@ void rs_tailfit(const double *hist802, int32_t cpsms, int32_t maxhyp, rs_result 
 void rs_traffic(const rs_length *lens, int nlen, const int32_t *moz, int npk, float prec, double dM,
                 const rs_params *par, int64_t *ids, int64_t *bins);
 
+/* Query preprocessing (source/core/msquery.cpp:338-423, keyval.h:49-129). */
+int32_t rs_cvt_i32(double v);
+int rs_pickpeaks(int32_t *mz, int32_t *in, int n_vec, int specsize, int32_t base_int, int32_t min_int, int qalen);
+
 #ifdef __cplusplus
 }
 #endif
+
 #endif
