@@ -67,6 +67,71 @@ def make_workload(name: str, rank: int):
     return w, db, H, q
 
 
+def prep_measure(gx, q, local: int, rank: int) -> dict:
+    """Peak picking of the workload's spectra as raw input (each spectrum's peaks shuffled,
+    intensities unnormalised, plus as many low noise peaks again), on the GPU
+    (gx_pickpeaks_device, CUDA events on its stream) and, on rank 0, the CPU baseline of
+    this step: the oracle's restatement on one host thread over a 2,000-spectrum sample.
+    Untimed set-up of the bench."""
+    import ctypes as C
+    import torch
+    import gicops_b200._native as N
+    rng = np.random.default_rng(77 + rank)
+    lens = np.diff(q.idx.astype(np.int64))
+    seg = np.zeros(q.n + 1, np.int64)
+    seg[1:] = np.cumsum(2 * lens)
+    n = int(seg[-1])
+    mz = np.empty(n, np.int32)
+    it = np.empty(n, np.int32)
+    for s in range(q.n):
+        a, b, k = int(q.idx[s]), int(q.idx[s + 1]), int(lens[s])
+        o = int(seg[s])
+        mz[o:o + k] = q.moz[a:b]
+        it[o:o + k] = (q.intn[a:b].astype(np.float64) * rng.uniform(0.5, 3.0)).astype(np.int32)
+        mz[o + k:o + 2 * k] = rng.integers(10000, 200000, k)
+        it[o + k:o + 2 * k] = rng.integers(0, 600, k)
+        perm = o + rng.permutation(2 * k)
+        mz[o:o + 2 * k], it[o:o + 2 * k] = mz[perm], it[perm]
+    d = torch.device("cuda", local)
+    t_seg = torch.from_numpy(seg.astype(np.int32)).to(d)
+    t_size = torch.from_numpy((2 * lens).astype(np.int32)).to(d)
+    t_mz0, t_it0 = torch.from_numpy(mz).to(d), torch.from_numpy(it).to(d)
+    t_mz, t_it = t_mz0.clone(), t_it0.clone()
+    o_idx = torch.empty(q.n + 1, dtype=torch.int32, device=d)
+    o_mz = torch.empty(max(n, 1), dtype=torch.int32, device=d)
+    o_it = torch.empty(max(n, 1), dtype=torch.int32, device=d)
+    st = torch.cuda.current_stream()
+    times = []
+    for rep in range(4):
+        t_mz.copy_(t_mz0)
+        t_it.copy_(t_it0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        N.check(N.lib().gx_pickpeaks_device(q.n, t_seg.data_ptr(), t_size.data_ptr(), t_mz.data_ptr(),
+                                            t_it.data_ptr(), 100000, 1000, 100, o_idx.data_ptr(), o_mz.data_ptr(),
+                                            o_it.data_ptr(), C.c_void_p(st.cuda_stream)))
+        e1.record(st)
+        st.synchronize()
+        if rep:
+            times.append(e0.elapsed_time(e1))
+    gpu_ms = float(np.median(times))
+    out = {"spectra": int(q.n), "raw_peaks": n, "gpu_ms": round(gpu_ms, 3),
+           "gpu_spectra_per_s": round(q.n / (gpu_ms / 1e3), 1)}
+    if rank == 0:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle
+        m = min(2000, q.n)
+        t1 = time.perf_counter()
+        idx, _, _ = pyoracle.pickpeaks(seg[:m + 1], 2 * lens[:m], mz, it)
+        cpu_s = time.perf_counter() - t1
+        out["cpu_baseline"] = {"value": round(m / cpu_s, 1), "unit": "spectra/s", "cores": 1, "kind": "port",
+                               "sample": f"first {m} spectra"}
+        out["kept_counts_equal_on_sample"] = bool(np.array_equal(
+            idx.astype(np.int64), o_idx[:m + 1].cpu().numpy().astype(np.int64)))
+    log(f"[bench] peak picking: {out['gpu_spectra_per_s']:.0f} spectra/s on the GPU")
+    return out
+
+
 def smi_id(local: int) -> str:
     vis = os.environ.get("CUDA_VISIBLE_DEVICES")
     if vis:
@@ -240,6 +305,7 @@ def main():
                        "host_threads": os.cpu_count()}
         log(f"[bench] index build: host {index_build['host_path_s']} s (build + upload), "
             f"device {index_build['device_path_s']} s (entries + GPU ions/CSR)")
+    prep = None if args.no_index_build else prep_measure(gx, q, local, rank)
     ws = gx.Searcher(dev, q.n, len(q.moz))
     stream = torch.cuda.current_stream()
     d = torch.device("cuda", local)
@@ -418,6 +484,7 @@ def main():
             "gpu_launches": launches,
             "path": "plain" if args.plain else ("batched+learned tail" if tail else "batched"),
             "index_build": index_build,
+            "prep": prep,
             "learned_tail": dict(tail_info or {}, queries_replaced=int(
                 ((t_out.cpu().numpy().view(N.RESULT_DTYPE)["status"] & N.STATUS_LEARNED_TAIL) != 0).sum()))
             if tail else None,
