@@ -16,6 +16,7 @@ LIB_PATH = os.path.join(HERE, "_lib", "libgicops_b200.so")
 
 HIST_BINS = 802
 MAX_HEAP = 31
+MAX_LENGTHS = 64
 MAX_PEAKS = 1024
 NOALLOC_MAX_WINDOWS = 1 << 19
 
@@ -121,6 +122,9 @@ _SIGS = [
     ("gx_index_build", C.c_int32, [C.POINTER(C.c_void_p), C.c_int32, C.POINTER(BuildParams), C.c_int32,
                                    C.POINTER(C.c_void_p)]),
     ("gx_index_read_length", C.c_int32, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("gx_merge_shards_device", C.c_int32, [C.c_uint32, C.c_int32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                           C.c_void_p, C.c_void_p, C.POINTER(Params), C.c_void_p, C.c_void_p,
+                                           C.c_void_p]),
     ("gx_ms2_read", C.c_int32, [C.c_char_p, C.c_uint32, C.POINTER(C.c_void_p)]),
     ("gx_ms2_desc", C.c_int32, [C.c_void_p, C.POINTER(Ms2Raw)]),
     ("gx_ms2_free", None, [C.c_void_p]),

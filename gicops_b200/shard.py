@@ -18,13 +18,18 @@ Two ways to spread a search over ranks:
   the tail fit then runs on the merged histogram, which equals the single-index one.
 
 The collectives go through torch.distributed (NCCL between GPUs; gloo for the CPU
-tests of this logic).
+tests of this logic).  ``merge_shards`` merges on the host; ``merge_shards_device``
+keeps everything on the GPU: the collectives run on CUDA tensors (NCCL) and the merge,
+the mapping to global length indices and the tail fit of the summed histograms run in
+one kernel (``gx_merge_shards_device``), which ``merge_gathered_device`` calls on
+already gathered data.
 """
 
 from __future__ import annotations
 
 import numpy as np
 
+from . import _native as N
 from ._native import CELL_DTYPE, HIST_BINS
 
 
@@ -111,3 +116,59 @@ def merge_shards(hist: np.ndarray, cpsms: np.ndarray, cells: np.ndarray, own_len
     allc = np.concatenate([p.numpy().reshape(-1).view(CELL_DTYPE).reshape(n, -1) for p in parts], axis=1)
     top = np.stack([merge_topk(allc[i], cap) for i in range(n)]) if n else np.zeros((0, cap), CELL_DTYPE)
     return h.numpy().astype(np.uint32).reshape(n, HIST_BINS), c.numpy().astype(np.int32), top
+
+
+def length_lut(own_lengths) -> np.ndarray:
+    """[GX_MAX_LENGTHS] global length index of each rank-local one (unused slots 0)."""
+    lut = np.zeros(N.MAX_LENGTHS, np.uint16)
+    lut[: len(own_lengths)] = np.asarray(own_lengths, dtype=np.uint16)
+    return lut
+
+
+def merge_gathered_device(params, cells, status, luts, hist, cpsms, stream=None):
+    """Merge of gathered shard results on the GPU (CUDA tensors, no collective):
+    cells uint8 [world, n, k*16] (gx_cell records, rank-local idxoffset), status int32
+    [world, n], luts uint16 [world, GX_MAX_LENGTHS], hist int32 [n, 802] and cpsms int32
+    [n] summed over ranks.  Returns (result records uint8 [n, record], top cells uint8
+    [n, cap*16]) on the same device."""
+    import ctypes as C
+    import torch
+    world, n = int(status.shape[0]), int(status.shape[1])
+    k = int(cells.shape[2]) // CELL_DTYPE.itemsize if n else 1
+    cap = int(N.lib().gx_heap_capacity(params.topmatches))
+    dev = cells.device
+    out = torch.empty((n, N.RESULT_DTYPE.itemsize), dtype=torch.uint8, device=dev)
+    top = torch.empty((n, cap * CELL_DTYPE.itemsize), dtype=torch.uint8, device=dev)
+    st = stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
+    cp = params.c() if hasattr(params, "c") else params
+    for t in (cells, status, luts, hist, cpsms):
+        assert t.is_contiguous() and t.device == dev
+    N.check(N.lib().gx_merge_shards_device(n, world, k, cells.data_ptr(), status.data_ptr(), luts.data_ptr(),
+                                           hist.data_ptr(), cpsms.data_ptr(), C.byref(cp), top.data_ptr(),
+                                           out.data_ptr(), C.c_void_p(st)))
+    return out, top
+
+
+def merge_shards_device(params, hist, cpsms, cells, status, own_lengths, world: int, group=None):
+    """Exchange + merge of the index-sharded search, on the GPU (every rank calls it, in
+    the same order): hist int32 [n, 802] and cpsms int32 [n] are this rank's partial
+    histograms and counts, cells uint8 [n, k*16] its top-k gx_cell records (rank-local
+    idxoffset), status int32 [n] its result statuses; all CUDA tensors.  One all_reduce of
+    histograms and counts, all_gathers of cells, statuses and length maps (NCCL), then
+    the device merge.  Returns (result records, top cells), identical on every rank."""
+    import torch
+    import torch.distributed as dist
+    dev = hist.device
+    h = hist.contiguous().clone()
+    c = cpsms.contiguous().clone()
+    dist.all_reduce(h, group=group)
+    dist.all_reduce(c, group=group)
+    lut = torch.from_numpy(length_lut(own_lengths).view(np.uint8)).to(dev)   # NCCL has no 16-bit ints: bytes
+    parts_c = [torch.empty_like(cells) for _ in range(world)]
+    parts_s = [torch.empty_like(status) for _ in range(world)]
+    parts_l = [torch.empty_like(lut) for _ in range(world)]
+    dist.all_gather(parts_c, cells.contiguous(), group=group)
+    dist.all_gather(parts_s, status.contiguous(), group=group)
+    dist.all_gather(parts_l, lut, group=group)
+    luts = torch.stack(parts_l).view(torch.int16)
+    return merge_gathered_device(params, torch.stack(parts_c), torch.stack(parts_s), luts, h, c)

@@ -224,6 +224,23 @@ typedef struct {
     double e_fp64;        /* e-value from the unquantized fit */
 } gx_result;
 
+/* ---- index-sharded search: merge of the ranks' partial results ----------------------
+ * Replaces the reference's exchange of partial results between MPI ranks that own
+ * peptide subsets (source/core/dslim_score.cpp:199-388, through files).  Every rank
+ * searched all nspec spectra against its own lengths (gx_search_device with heap and
+ * histogram outputs); after the histograms and candidate counts are summed over ranks
+ * and the ranks' cells and statuses gathered (NCCL), this writes the global top cells
+ * [nspec][cap] (cap = gx_heap_capacity(p->topmatches); top_dev may be NULL) ordered by
+ * hyperscore descending, then global length index and entry ascending, and the result
+ * records with the tail fit of the summed histogram.  cells_dev [world][nspec][k] with
+ * rank-local idxoffset, status_dev [world][nspec], lut_dev [world][GX_MAX_LENGTHS] =
+ * global length index of each rank-local one, hist_dev [nspec][GX_HIST_BINS] and
+ * cpsms_dev [nspec] summed.  Stream-ordered. */
+gx_status gx_merge_shards_device(uint32_t nspec, int32_t world, uint32_t k, const gx_cell *cells_dev,
+                                 const int32_t *status_dev, const uint16_t *lut_dev, const uint32_t *hist_dev,
+                                 const int32_t *cpsms_dev, const gx_params *p, gx_cell *top_dev, gx_result *out_dev,
+                                 void *stream);
+
 /* Workspace sized for up to max_spec spectra / max_peaks peaks per call. */
 gx_status gx_workspace_create(const gx_index *ix, uint32_t max_spec, uint32_t max_peaks, gx_workspace **out);
 gx_status gx_workspace_free(gx_workspace *ws);
