@@ -180,8 +180,15 @@ __global__ void __launch_bounds__(kPrepBlock) k_prep(SearchArgs a, int2 *win, ui
 #endif
 constexpr int kBWarps = GX_BATCH_WARPS;      // warps per CTA
 constexpr int kBBlock = kBWarps * 32;
-constexpr int kCtasPerSm = 1024 / kBBlock;   // resident CTAs per SM (each its own spectrum)
-constexpr int kPend = 160;      // per-warp queue of candidates awaiting a hyperscore (32 + one scan step)
+#ifndef GX_CTAS_PER_SM
+#define GX_CTAS_PER_SM (1024 / (GX_BATCH_WARPS * 32))
+#endif
+constexpr int kCtasPerSm = GX_CTAS_PER_SM;   // resident CTAs per SM (each its own spectrum)
+#ifndef GX_PEND
+#define GX_PEND 160
+#endif
+constexpr int kPend = GX_PEND;  // per-warp queue of candidates awaiting a hyperscore (32 + one scan step)
+static_assert(kPend >= 128, "the queue must hold one scan step's candidates (32 lanes x 4)");
 constexpr int kIvlChunk = 256;  // intervals per span table
 constexpr int kDummy = 32;      // scorecard words that take the adds of ids outside the tile (one per lane)
 #ifndef GX_STREAM_CHUNKS
@@ -189,7 +196,10 @@ constexpr int kDummy = 32;      // scorecard words that take the adds of ids out
 #endif
 constexpr int kChunks = GX_STREAM_CHUNKS;   // 16-byte id chunks in flight per lane
 constexpr int kHeapWarp = kBWarps - 1;      // inserts heap entrants while the others stream
-constexpr int kEntSmem = 8;     // heap entrants per warp kept in shared memory
+#ifndef GX_ENT_SMEM
+#define GX_ENT_SMEM 8
+#endif
+constexpr int kEntSmem = GX_ENT_SMEM;   // heap entrants per warp kept in shared memory
 
 // Dynamic shared memory after the scorecard tile (tile * 8 bytes):
 //   dummy      kDummy words right after the scorecard, written and never read
