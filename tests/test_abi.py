@@ -70,3 +70,21 @@ def test_search_params_roundtrip():
     c = p.c()
     assert (c.dM, c.dF, c.topmatches, c.scale) == (500.0, 5, 10, 100)
     assert p.heap_cap == 15
+
+
+def test_merge_and_prep_argument_checks():
+    """gx_merge_shards_device and gx_pickpeaks_device reject bad arguments on the host,
+    before any device call."""
+    L = N.lib()
+    p = gx.SearchParams().c()
+    dummy = 16   # never dereferenced: every call below fails its host-side checks
+    assert L.gx_merge_shards_device(4, 2, 7, None, dummy, dummy, dummy, dummy, C.byref(p), None, dummy, None) == -3008
+    assert L.gx_merge_shards_device(4, 0, 7, dummy, dummy, dummy, dummy, dummy, C.byref(p), None, dummy, None) == -3002
+    assert L.gx_merge_shards_device(4, 2, 0, dummy, dummy, dummy, dummy, dummy, C.byref(p), None, dummy, None) == -3002
+    assert L.gx_merge_shards_device(4, 2, 32, dummy, dummy, dummy, dummy, dummy, C.byref(p), None, dummy, None) == -3002
+    p1 = gx.SearchParams(topmatches=1).c()                       # heap capacity 0
+    assert L.gx_merge_shards_device(4, 2, 7, dummy, dummy, dummy, dummy, dummy, C.byref(p1), None, dummy, None) == -3002
+    assert L.gx_merge_shards_device(4, 2, 7, dummy, dummy, dummy, dummy, dummy, None, None, dummy, None) == -3008
+    assert L.gx_pickpeaks_device(1 << 31, dummy, dummy, dummy, dummy, 100000, 1000, 100, dummy, dummy, dummy,
+                                 None) == -3004
+    assert b"gx_pickpeaks_device" in L.gx_last_error()
