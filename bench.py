@@ -46,6 +46,12 @@ WORKLOADS = {
                              npeaks_range=(30, 150), window="mixed")),
     "closed-1k": dict(nproteins=1000, db_seed=1, maxz=1, mods=[], nmods=0, nspec=2000, dM=10.0,
                       q=dict(charges=(2, 3), frag_charge2=False, keep_p=(0.6, 0.6), noise_mode="fixed40")),
+    # the large config at its stated size: 200,000 proteins, Met oxidation <= 3 (39.7M entries,
+    # 3.3G ion ids), 200,000 spectra, half +-10 ppm and half +-500 Da, 20-80% ion retention
+    # (the N-terminal acetylation of that config cannot be expressed in the reference: left out)
+    "large-200k": dict(nproteins=200000, db_seed=1, maxz=2, mods=[("M", 15.9949, 3)], nmods=3, nspec=200000,
+                       dM=500.0, q=dict(charges=(2, 4), frag_charge2=True, keep_p=(0.2, 0.8), noise_mode="fill",
+                                        npeaks_range=(30, 150), window="mixed")),
 }
 
 
