@@ -68,6 +68,9 @@ def test_gpu_golden(gx, golden, case, flags):
     r = s.search(q, search_params(c, flags=flags), heap=True, hist=True)
     ores, ohist = pyoracle.search(H.lengths, q, oracle_params(c), hist=True)
     assert_same(r.result, r.heap, r.hist, ores, ohist, c)
+    # no shared-ion count above MAX_SHDPEAKS (80) on the configs: the reference would read
+    # past its lgfact table there (utils.h:110, dslim_query.cpp:936); status bit 4 flags it
+    assert not np.any(r.result["status"] & 4)
     if flags == 1:
         assert np.all((r.result["status"] & 8) != 0)
 
@@ -95,6 +98,7 @@ def test_gpu_random_open_search(gx, seed):
     r = s.search(q, p, heap=True, hist=True)
     ores, ohist = pyoracle.search(H.lengths, q, pyoracle.Params(dM=500.0), hist=True)
     assert_same(r.result, r.heap, r.hist, ores, ohist, None)
+    assert not np.any(r.result["status"] & 4)
 
 
 def test_gpu_topmatches_and_min_shp(gx, golden):
