@@ -200,6 +200,9 @@ constexpr int kHeapWarp = kBWarps - 1;      // inserts heap entrants while the o
 #define GX_ENT_SMEM 8
 #endif
 constexpr int kEntSmem = GX_ENT_SMEM;   // heap entrants per warp kept in shared memory
+#ifndef GX_FUSED_CLEAR
+#define GX_FUSED_CLEAR 1   // packed scorecard reset during the scan and after scoring (0: one pass after)
+#endif
 
 // Dynamic shared memory after the scorecard tile (tile * 8 bytes):
 //   dummy      kDummy words right after the scorecard, written and never read
@@ -357,6 +360,17 @@ __device__ __forceinline__ void score_batch(BatchSmem &sm, const BatchDyn &dd, c
         }
         nent += __popc(eb);
     }
+    }
+}
+
+// Resets the packed-scorecard groups (four candidates, 32 bytes) of the n scored
+// candidates in q: the scan left every group holding a PSM as it was, for the scoring.
+__device__ __forceinline__ void clear_scored(uint32_t *sw, const uint32_t *q, int n, int lane)
+{
+    for (int i = lane; i < n; i += 32) {
+        uint4 *z = reinterpret_cast<uint4 *>(sw + 2 * (q[i] & ~3u));
+        z[0] = make_uint4(0u, 0u, 0u, 0u);
+        z[1] = make_uint4(0u, 0u, 0u, 0u);
     }
 }
 
@@ -760,6 +774,13 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
                                 ((((qa.z >> 24) + (qa.w >> 24)) >= minshp && lim4 > 1) ? 2u : 0u) |
                                 ((((qb.x >> 24) + (qb.y >> 24)) >= minshp && lim4 > 2) ? 4u : 0u) |
                                 ((((qb.z >> 24) + (qb.w >> 24)) >= minshp && lim4 > 3) ? 8u : 0u);
+#if GX_FUSED_CLEAR
+                            if (m == 0u) {   // no PSM among the four: reset them for the next tile now
+                                uint4 *z = reinterpret_cast<uint4 *>(sw + 2 * cb);
+                                z[0] = make_uint4(0u, 0u, 0u, 0u);
+                                z[1] = make_uint4(0u, 0u, 0u, 0u);
+                            }
+#endif
                         }
                     } else {
                         cb = c0 + lane;
@@ -777,6 +798,8 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
                     if (npend + total > kPend) {   // queue full: score what it holds first
                         __syncwarp();
                         score_batch(sm, dd, a, scv, ctile, wid, lane, npend, t0, ixx, speclen, tau, wide, ent, nent, cps);
+                        __syncwarp();
+                        if (!wide) clear_scored(sw, dd.pend[wid], npend, lane);
                         npend = 0;
                         __syncwarp();
                     }
@@ -785,19 +808,25 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
                     npend += total;
                 }
                 __syncwarp();
-                if (npend > 0)
+                if (npend > 0) {
                     score_batch(sm, dd, a, scv, ctile, wid, lane, npend, t0, ixx, speclen, tau, wide, ent, nent, cps);
+                    __syncwarp();
+                    if (!wide) clear_scored(sw, dd.pend[wid], npend, lane);
+                }
                 if (lane == 0) {
                     sm.warp_cnt[wid] = nent;
                     if (nent) atomicOr(&sm.ent_mask, 1u << wid);
                 }
                 // clear the warp's range [r0, r1) of every array (rounded up to 4 words: the
-                // next range starts at a multiple of 32, the arrays end at one)
+                // next range starts at a multiple of 32, the arrays end at one); the packed
+                // scorecard was reset during the scan and after scoring
                 __syncwarp();
                 if (r0 < r1) {
                     if (!wide) {   // words [2 r0, 2 r1), two candidates per 16 bytes
-                        uint4 *z = reinterpret_cast<uint4 *>(sw);
-                        for (int i = r0 / 2 + lane; i < (r1 + 1) / 2; i += 32) z[i] = make_uint4(0u, 0u, 0u, 0u);
+                        if (!GX_FUSED_CLEAR) {
+                            uint4 *z = reinterpret_cast<uint4 *>(sw);
+                            for (int i = r0 / 2 + lane; i < (r1 + 1) / 2; i += 32) z[i] = make_uint4(0u, 0u, 0u, 0u);
+                        }
                     } else {
                         const int q0 = r0 >> 2, q1 = min(ctile, (r1 + 3) & ~3) >> 2;
                         for (int k = 0; k < 3; k++) {
