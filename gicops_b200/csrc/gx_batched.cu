@@ -799,7 +799,7 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
                         __syncwarp();
                         score_batch(sm, dd, a, scv, ctile, wid, lane, npend, t0, ixx, speclen, tau, wide, ent, nent, cps);
                         __syncwarp();
-                        if (!wide) clear_scored(sw, dd.pend[wid], npend, lane);
+                        if (!wide && GX_FUSED_CLEAR) clear_scored(sw, dd.pend[wid], npend, lane);
                         npend = 0;
                         __syncwarp();
                     }
@@ -811,7 +811,7 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
                 if (npend > 0) {
                     score_batch(sm, dd, a, scv, ctile, wid, lane, npend, t0, ixx, speclen, tau, wide, ent, nent, cps);
                     __syncwarp();
-                    if (!wide) clear_scored(sw, dd.pend[wid], npend, lane);
+                    if (!wide && GX_FUSED_CLEAR) clear_scored(sw, dd.pend[wid], npend, lane);
                 }
                 if (lane == 0) {
                     sm.warp_cnt[wid] = nent;
