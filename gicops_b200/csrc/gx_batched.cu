@@ -200,6 +200,10 @@ constexpr int kHeapWarp = kBWarps - 1;      // inserts heap entrants while the o
 #define GX_ENT_SMEM 8
 #endif
 constexpr int kEntSmem = GX_ENT_SMEM;   // heap entrants per warp kept in shared memory
+#ifndef GX_WARP_SEARCH
+#define GX_WARP_SEARCH 1   // a unit's first interval found by a two-level warp search (0: binary search)
+#endif
+static_assert(kIvlChunk <= 256, "the warp search covers 32 x 8 span-table entries");
 #ifndef GX_FUSED_CLEAR
 #define GX_FUSED_CLEAR 1   // packed scorecard reset during the scan and after scoring (0: one pass after)
 #endif
@@ -546,12 +550,24 @@ __device__ __forceinline__ void stream_tile(BatchSmem &sm, const BatchDyn &dd, c
         u = __shfl_sync(0xffffffffu, u, 0);
         const uint32_t j0 = u * (32u * kChunks);
         if (j0 >= M) break;
-        // interval of the unit's first chunk; each lane walks on from there
+        // interval of the unit's first chunk (the last k < ncv with pre[k] <= j0, a non-empty
+        // interval: pre is non-decreasing, pre[0] = 0 and pre[ncv] > j0); each lane walks on
+        // from there
+#if GX_WARP_SEARCH
+        // two levels across the warp: every 8th entry, then the 8 entries of that group
+        const uint32_t s1 = (uint32_t)lane * 8u;
+        const uint32_t b1 = __ballot_sync(0xffffffffu, s1 < ncv && dd.sp_pre[s1] <= j0);
+        const uint32_t base = (31u - (uint32_t)__clz(b1)) * 8u;
+        const uint32_t s2 = base + ((uint32_t)lane & 7u);
+        const uint32_t b2 = __ballot_sync(0xffffffffu, lane < 8 && s2 < ncv && dd.sp_pre[s2] <= j0);
+        uint32_t k = base + (31u - (uint32_t)__clz(b2));
+#else
         uint32_t k = 0, hi = ncv;
         while (hi - k > 1) {
             const uint32_t mid = (k + hi) >> 1;
             if (dd.sp_pre[mid] <= j0) k = mid; else hi = mid;
         }
+#endif
         uint4 v[kChunks];
         uint32_t kx[kChunks];
 #pragma unroll
