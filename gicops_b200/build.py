@@ -26,6 +26,10 @@ HOSTCXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "--expt-relaxed-constexpr",
            "-Xcompiler", "-fPIC,-fopenmp,-ffp-contract=off", "-ccbin", HOSTCXX, "-I" + os.path.join(ROOT, "include")]
+# extra nvcc flags, e.g. GX_NVCC_FLAGS="-DGX_STREAM_CHUNKS=3" (recorded next to the library, so
+# that a change of flags rebuilds it)
+EXTRA = os.environ.get("GX_NVCC_FLAGS", "").split()
+STAMP = os.path.join(OUT, "nvcc_flags.txt")
 CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-fopenmp", "-ffp-contract=off", "-I" + os.path.join(ROOT, "include")]
 
 
@@ -41,6 +45,8 @@ def _deps():
 def up_to_date() -> bool:
     if not os.path.exists(LIB):
         return False
+    if (open(STAMP).read() if os.path.exists(STAMP) else "") != " ".join(EXTRA):
+        return False
     t = os.path.getmtime(LIB)
     return all(os.path.getmtime(p) <= t for p in _deps())
 
@@ -53,7 +59,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     for src in sources():
         obj = os.path.join(OUT, "obj", os.path.basename(src) + ".o")
         if src.endswith(".cu"):
-            cmd = [NVCC, *ARCH, *CUFLAGS, "-c", src, "-o", obj]
+            cmd = [NVCC, *ARCH, *CUFLAGS, *EXTRA, "-c", src, "-o", obj]
         else:
             cmd = [HOSTCXX, *CXXFLAGS, "-c", src, "-o", obj]
         if verbose:
@@ -67,6 +73,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)
     shutil.move(tmp, LIB)
+    with open(STAMP, "w") as f:
+        f.write(" ".join(EXTRA))
     return LIB
 
 
