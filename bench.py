@@ -1,23 +1,29 @@
 """Benchmark of the peptide-search query path (spectra/s) on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload open-20k] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload large-200k] [--impl ours|reference]
 
-A step is one search of the whole synthetic batch (default: the open-search
-workload -- 20,000 proteins, Met oxidation <= 2, b/y ions of charge 1-2, 50,000
-spectra of 30-150 peaks, +-500 Da precursor window, +-0.05 Da fragment tolerance,
-top-K 5).  Its index (2.8 GB) is larger than L2, so steps run back to back; an
-index smaller than twice L2 (the closed-1k workload's) is flushed from L2 before each
-timed step instead, and the step timed alone.
+A step is one search of the whole synthetic batch.  The default workload is the large
+open-search configuration: 200,000 proteins with Met oxidation <= 3 (39.7M index entries,
+3.3G fragment-ion ids, b/y ions of charge 1-2, a 27 GB index in HBM), 200,000 spectra of
+30-150 peaks with 20-80% ion retention, half at a +-10 ppm and half at a +-500 Da precursor
+window, +-0.05 Da fragment tolerance, top-K 5.  Its index is larger than L2, so steps run
+back to back; an index smaller than twice L2 (the closed-1k workload's) is flushed from L2
+before each timed step instead, and the step timed alone.
 
-Printed (rank 0, one JSON line): value = spectra/s with queries resident in HBM
-(CUDA events on the launching stream, max over ranks); e2e = spectra/s through
-the host-buffer API (pinned host queries in, results out, per step); roofline of
-the dominant kernel against the measured HBM copy bandwidth; cpu_baseline = the
-reference's own OpenMP CPU query path timed on a bounded sample on this host.
+Printed (rank 0, one JSON line): value = spectra/s with queries resident in HBM (CUDA
+events on the launching stream, max over ranks); e2e = spectra/s through the host-buffer
+API (pinned host queries in, results out, per step); roofline of the dominant kernel
+against the measured HBM copy bandwidth; parity = the benchmarked batch's own outputs
+against the oracle on a seeded sample, with the accuracy figures; plain_path = the plain
+one-spectrum-per-CTA path on a seeded sample, beside the batched path on the same sample;
+cpu_baseline = the reference's own OpenMP CPU query path timed on a bounded sample on
+this host.
 
 Under torchrun each rank searches its own batch against a replica of the index
 (spectra are independent: weak scaling, no collective on the data path).
-``--impl reference`` times the reference's CPU implementation alone (rank 0).
+``--impl reference`` times the reference's CPU implementation alone (rank 0); that arm
+runs the compiled reference and numpy only (its queries come from the reference's own
+index entries), and loads nothing of this package's native library.
 """
 
 from __future__ import annotations
@@ -56,8 +62,55 @@ WORKLOADS = {
 }
 
 
+# spectra per step of the reference's CPU path: a seeded random subset of the workload's
+# batch (the whole batch where it takes seconds), sized for a few seconds per step
+REF_SAMPLE = {"large-200k": 1024, "mixed-20k": 4096, "open-20k": 2048, "closed-1k": 2000}
+
+
 def log(*a):
     print(*a, file=sys.stderr, flush=True)
+
+
+def ref_sample(name: str, n: int) -> np.ndarray:
+    """The seeded subset of the batch that the reference's CPU path is timed on (both arms)."""
+    m = min(n, REF_SAMPLE.get(name, 2048))
+    sel = np.random.Generator(np.random.PCG64(7)).choice(n, size=m, replace=False)
+    sel.sort()
+    return sel
+
+
+def make_reference_workload(name: str):
+    """The workload for the reference arm, with no call into this package's native library:
+    the database from the seeded generator (numpy), the index entries (peptides and Met-ox
+    variants in index order) from the compiled reference itself (ref_harness
+    --entries-only), and the spectra drawn from those entries by the same generator and
+    seed as rank 0 of the GPU arm (the two sets of entries are identical: the library's
+    builder is pinned to the reference's arrays)."""
+    from gicops_b200 import synth
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import refdump
+    w = WORKLOADS[name]
+    t = time.time()
+    db = synth.make_database(w["nproteins"], seed=w["db_seed"])
+    with tempfile.TemporaryDirectory() as tmp:
+        dbdir = os.path.join(tmp, "db")
+        db.write_peps(dbdir)
+        dump = os.path.join(tmp, "entries.bin")
+        cmd = [os.path.join(ROOT, "oracle", "_ref", "ref_harness"), "--db", dbdir, "--maxz", str(w["maxz"]),
+               "--entries-only", "--dump-index", dump]
+        for r, m, n in w["mods"]:
+            cmd += ["--mods", f"{r}:{m}:{n}"]
+        if w["mods"]:
+            cmd += ["--nmods", str(w["nmods"])]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"reference harness failed: {r.stderr[-400:]}")
+        _, R = refdump.read_index_dump(dump)
+    ent = {x["L"]: (x["seqs"], x["seqid"], x["sites"], x["mass"]) for x in R if x["N"]}
+    q = synth.make_queries(ent, w["nspec"], seed=1000, **w["q"])
+    log(f"[bench] reference workload {name}: {sum(x['N'] for x in R)} entries (reference build), {q.n} spectra "
+        f"({time.time() - t:.1f}s)")
+    return w, db, q
 
 
 def make_workload(name: str, rank: int):
@@ -202,17 +255,14 @@ def _harness_run(w: dict, db, sq, steps: int, warmup: int, cores: int, dM: float
     return rec["query_s_each"][warmup:]
 
 
-def reference_cpu(w: dict, db, q, steps: int, warmup: int, sample: int | None = None):
-    """The reference's OpenMP CPU query path (oracle/_ref/ref_harness) on a sample of q.
+def reference_cpu(w: dict, db, q, sel, steps: int, warmup: int):
+    """The reference's OpenMP CPU query path (oracle/_ref/ref_harness) on the spectra sel of q.
 
     The reference reads one global precursor tolerance, so a batch with per-spectrum
     tolerances is timed in two batches: the spectra at the workload's window, and the
     narrow-window spectra at the median of their tolerances (timing only)."""
     cores = os.cpu_count() or 1
-    if sample is None:
-        sample = int(min(q.n, max(2048, min(16384, 128 * cores))))
-    sel = np.random.Generator(np.random.PCG64(7)).choice(q.n, size=sample, replace=False)
-    sel.sort()
+    sample = len(sel)
     sq = q.subset(sel)
     if sq.dM is None or np.all(np.isnan(sq.dM)):
         each = _harness_run(w, db, sq, steps, warmup, cores, w["dM"])
@@ -232,16 +282,98 @@ def reference_cpu(w: dict, db, q, steps: int, warmup: int, sample: int | None = 
     return dict(value=sample / per, cores=cores, sample=sample, seconds=per, steps=len(each))
 
 
+def parity_block(gx, N, H, q, params, w, run_full, tail_on: bool, n_sample: int = 256, n_hyp: int = 32) -> dict:
+    """Untimed check of the benchmarked batch's own outputs: one more search of the whole
+    batch (the timed step's launch sequence, with heap and histogram outputs) against the
+    oracle on a seeded sample of its spectra.  Exact: candidate counts, histograms, heap
+    arrays, top PSMs, and the tail fit of every query that kept the plain fit; FP64 slope
+    and e-value to 1e-12 / 1e-9 relative.  Accuracy: the top PSMs' FP32 hyperscores
+    against FP64 (n_hyp spectra), the reference's quantized e-value against the
+    unquantized FP64 fit, and the learned tail's e-values against the plain FP64 fit of
+    the same histograms (every query of the batch that took it)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    rng = np.random.Generator(np.random.PCG64(3))
+    sel = np.sort(rng.choice(q.n, size=min(q.n, n_sample), replace=False))
+    res_all, heap, hist = run_full(sel)
+    res = res_all[sel]
+    sq = q.subset(sel)
+    t0 = time.perf_counter()
+    o, oh = pyoracle.search(H.lengths, sq, pyoracle.Params(dM=w["dM"], topmatches=params.topmatches,
+                                                           expect_max=params.expect_max), hist=True)
+    oracle_s = time.perf_counter() - t0
+    learned = (res["status"] & N.STATUS_LEARNED_TAIL) != 0
+    fitted = (o["status"] & 1) != 0
+    heaps_ok = True
+    for i in range(len(sel)):
+        k = int(o["heap_size"][i])
+        a_, b_ = heap[i][:k], o["heap"][i][:k]
+        heaps_ok &= bool(np.array_equal(a_["psid"], b_["psid"]) and np.array_equal(a_["idxoffset"], b_["idxoffset"])
+                         and np.array_equal(a_["sharedions"], b_["sharedions"])
+                         and np.array_equal(a_["hyperscore"].view(np.uint32), b_["hyperscore"].view(np.uint32)))
+    top_ok = all(np.array_equal(res["top"][f][fitted], o["top"][f][fitted])
+                 for f in ("psid", "idxoffset", "sharedions", "totalions")) and \
+        np.array_equal(res["top"]["hyperscore"][fitted].view(np.uint32), o["top"]["hyperscore"][fitted].view(np.uint32))
+    plain = fitted & ~learned
+    fit_ok = all(np.array_equal(res[f][plain], o[f][plain]) for f in ("maxhyp", "mu", "beta", "stt1", "end1")) and \
+        np.array_equal(res["status"][plain] & 7, o["status"][plain] & 7) and \
+        np.array_equal(res["status"][learned] & 5, o["status"][learned] & 5)
+    fin = fitted & np.isfinite(o["e_fp64"]) & (o["e_fp64"] > 0)
+    rel = lambda x, y: float(np.max(np.abs(x - y) / np.maximum(np.abs(y), 1e-300))) if len(y) else 0.0  # noqa: E731
+    e_rel = rel(res["e_x"][plain & fin], o["e_x"][plain & fin])
+    fp64_rel = rel(res["e_fp64"][fin], o["e_fp64"][fin])
+    slope_rel = rel(res["slope"][fin], o["slope"][fin])
+    # hyperscore of the top PSM in FP32 against its FP64 value (oracle scorecard of the spectrum)
+    lg = pyoracle.lgfact()
+    hyp_err = 0.0
+    for i in np.nonzero(fitted)[0][:n_hyp]:
+        a0, a1 = int(sq.idx[i]), int(sq.idx[i + 1])
+        dm = w["dM"] if sq.dM is None or np.isnan(sq.dM[i]) else float(sq.dM[i])
+        c = pyoracle.candidates(H.lengths, sq.moz[a0:a1], sq.intn[a0:a1], float(sq.prec[i]), dm,
+                                pyoracle.Params(dM=dm), cap=1 << 23)
+        t = res["top"][i]
+        m = c[(c["ixx"] == t["idxoffset"]) & (c["psid"] == t["psid"])]
+        if len(m):
+            bc, yc = min(int(m["bc"][0]), 80), min(int(m["yc"][0]), 80)
+            h64 = lg[bc] + lg[yc] + np.log10(1.0 + float(m["ibc"][0])) + np.log10(1.0 + float(m["iyc"][0])) - 4.0
+            hyp_err = max(hyp_err, abs(float(t["hyperscore"]) - h64) / abs(h64))
+    # the reference's e-value (slope/intercept truncated to 1e-6) against the unquantized fit
+    q_fit = plain & fin & (res["e_x"] > 0)
+    dq = np.abs(np.log10(res["e_x"][q_fit]) - np.log10(o["e_fp64"][q_fit])) if q_fit.any() else np.zeros(1)
+    out = {"sample": int(len(sel)), "sample_seed": 3, "oracle_s": round(oracle_s, 2),
+           "cpsms_equal": bool(np.array_equal(res["cpsms"], o["cpsms"])),
+           "histograms_equal": bool(np.array_equal(hist, oh)), "heaps_equal": bool(heaps_ok),
+           "top_psm_equal": bool(top_ok), "tail_fit_equal": bool(fit_ok),
+           "e_x_max_rel_err": e_rel, "e_fp64_max_rel_err": fp64_rel, "slope_max_rel_err": slope_rel,
+           "hyperscore_fp32_vs_fp64_max_rel_err": hyp_err, "hyperscore_spectra": int(min(n_hyp, fitted.sum())),
+           "e_quantized_vs_fp64_log10": {"median": float(np.median(dq)), "max": float(np.max(dq))},
+           "fitted_in_sample": int(fitted.sum())}
+    if tail_on:
+        L = ((res_all["status"] & N.STATUS_LEARNED_TAIL) != 0) & (res_all["e_x"] > 0) & (res_all["e_fp64"] > 0)
+        d = np.abs(np.log10(res_all["e_x"][L]) - np.log10(res_all["e_fp64"][L])) if L.any() else np.zeros(0)
+        out["learned_tail_vs_plain_fit"] = {
+            "queries": int(L.sum()),
+            "share_within_0.1_log10": float(np.mean(d <= 0.1)) if len(d) else None,
+            "median_abs_log10": float(np.median(d)) if len(d) else None}
+    out["all_exact"] = bool(out["cpsms_equal"] and out["histograms_equal"] and out["heaps_equal"] and
+                            out["top_psm_equal"] and out["tail_fit_equal"] and e_rel <= 1e-9 and fp64_rel <= 1e-9)
+    log(f"[bench] parity on {len(sel)} sampled spectra: exact={out['all_exact']} (oracle {oracle_s:.1f}s)")
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="open-20k", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="large-200k", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain", action="store_true", help="time the plain one-spectrum-per-CTA path instead")
-    ap.add_argument("--compare-plain", action="store_true", help="also time one step of the plain path")
+    ap.add_argument("--plain-sample", type=int, default=4096,
+                    help="spectra of the seeded sample the plain path is timed on (0: leave it out)")
+    ap.add_argument("--parity-sample", type=int, default=256,
+                    help="spectra of the seeded sample checked against the oracle (0: leave it out)")
     ap.add_argument("--spectra", type=int, default=0, help="search only the first N spectra (profiling cases)")
     ap.add_argument("--no-tail", action="store_true", help="leave the learned tail out of the step")
     ap.add_argument("--no-index-build", action="store_true", help="skip timing the GPU index build at set-up")
@@ -259,14 +391,17 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        w, db, H, q = make_workload(args.workload, 0)
-        ref = reference_cpu(w, db, q, args.steps, args.warmup)
+        w, db, q = make_reference_workload(args.workload)
+        sel = ref_sample(args.workload, q.n)
+        ref = reference_cpu(w, db, q, sel, args.steps, args.warmup)
         line = {"metric": metric, "value": ref["value"], "unit": unit, "impl": "reference", "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ref["seconds"] * 1e3,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32+f64",
                 "data": "synthetic (seeded generator)",
                 "config": {"workload": args.workload, "spectra_per_step": ref["sample"],
-                           "window_da": w["dM"] if q.dM is None else "half +-10 ppm, half +-%g Da" % w["dM"]},
+                           "window_da": w["dM"] if q.dM is None else "half +-10 ppm, half +-%g Da" % w["dM"],
+                           "sample": f"seeded subset (PCG64 seed 7) of the workload's {w['nspec']} spectra, "
+                                     "the same subset the GPU arm's cpu_baseline times"},
                 "cpu_baseline": {"value": ref["value"], "unit": unit, "cores": ref["cores"], "kind": "reference",
                                  "sample": f"{ref['sample']} of the workload's {w['nspec']} spectra per step"},
                 "e2e": {"value": ref["value"], "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -293,10 +428,11 @@ def main():
     t1 = time.perf_counter()
     dev = gx.DeviceIndex(H, local)
     upload_s = time.perf_counter() - t1
+    extras = world == 1   # set-up measurements beside the step: one process only
     # ---- index build: the same index with its fragment ions, CSR and block layout computed
     # on the GPU (entries on the host), against the host build + upload above (untimed setup)
     index_build = None
-    if not args.no_index_build:
+    if extras and not args.no_index_build:
         t1 = time.perf_counter()
         E = gx.HostIndex.build(db, maxz=w["maxz"], mods=w["mods"], nmods=w["nmods"], ions=False)
         entries_s = time.perf_counter() - t1
@@ -312,22 +448,24 @@ def main():
                        "host_threads": os.cpu_count()}
         log(f"[bench] index build: host {index_build['host_path_s']} s (build + upload), "
             f"device {index_build['device_path_s']} s (entries + GPU ions/CSR)")
-    prep = None if args.no_index_build else prep_measure(gx, q, local, rank)
+    prep = prep_measure(gx, q, local, rank) if extras and not args.no_index_build else None
     ws = gx.Searcher(dev, q.n, len(q.moz))
     stream = torch.cuda.current_stream()
     d = torch.device("cuda", local)
-    t_idx = torch.from_numpy(q.idx.view(np.int32).copy()).to(d)
-    t_moz = torch.from_numpy(q.moz.copy()).to(d)
-    t_int = torch.from_numpy(q.intn.copy()).to(d)
-    t_pre = torch.from_numpy(q.prec.copy()).to(d)
-    t_chg = torch.from_numpy(q.charge.astype(np.int32)).to(d)
+
+    def device_queries(qq):
+        t = dict(idx=torch.from_numpy(qq.idx.view(np.int32).copy()).to(d), moz=torch.from_numpy(qq.moz.copy()).to(d),
+                 intn=torch.from_numpy(qq.intn.copy()).to(d), prec=torch.from_numpy(qq.prec.copy()).to(d),
+                 charge=torch.from_numpy(qq.charge.astype(np.int32)).to(d))
+        if qq.dM is not None:   # per-spectrum precursor tolerances (Da)
+            t["dM"] = torch.from_numpy(np.where(np.isnan(qq.dM), w["dM"], qq.dM).astype(np.float64)).to(d)
+        qd_ = dict(nspec=qq.n, npeaks=len(qq.moz), **{k: v.data_ptr() for k, v in t.items()})
+        return qd_, t
+
+    qd, qt = device_queries(q)
+    t_pre, t_chg = qt["prec"], qt["charge"]
     t_out = torch.empty(q.n * N.RESULT_DTYPE.itemsize, dtype=torch.uint8, device=d)
     t_hist = torch.empty((q.n, N.HIST_BINS), dtype=torch.int32, device=d)
-    qd = dict(nspec=q.n, npeaks=len(q.moz), idx=t_idx.data_ptr(), moz=t_moz.data_ptr(), intn=t_int.data_ptr(),
-              prec=t_pre.data_ptr(), charge=t_chg.data_ptr())
-    if q.dM is not None:   # per-spectrum precursor tolerances (Da)
-        t_dm = torch.from_numpy(np.where(np.isnan(q.dM), w["dM"], q.dM).astype(np.float64)).to(d)
-        qd["dM"] = t_dm.data_ptr()
 
     # ---- learned tail: trained here (untimed) on this workload's well-populated queries --
     tail = None
@@ -356,7 +494,6 @@ def main():
         else:
             tail = None
         log(f"[bench] learned tail: {tail_info}")
-    del t_hist
 
     def step():
         ws.search_device(qd, params, t_out.data_ptr(), stream=stream.cuda_stream)
@@ -407,8 +544,9 @@ def main():
     value = q.n * world / (ms_step / 1e3)
 
     # ---- dominant kernel duration (events around each launch, same stream) --------
+    prof_steps = min(args.steps, 3)
     gx.lib().gx_profile_enable(1)
-    for _ in range(args.steps):
+    for _ in range(prof_steps):
         step()
     torch.cuda.synchronize()
     kt = N.kernel_times()
@@ -420,12 +558,13 @@ def main():
     # queries copied in, search, learned tail when attached, results copied out) ------
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
     qp = gx.synth.QueryBatch(pin(q.idx), pin(q.moz), pin(q.intn), pin(q.prec), pin(q.charge.astype(np.int32)),
-                             q.rtime, q.dM)
+                             q.rtime, None if q.dM is None else pin(np.where(np.isnan(q.dM), w["dM"], q.dM)))
     out_pinned = torch.empty(q.n * N.RESULT_DTYPE.itemsize, dtype=torch.uint8).pin_memory().numpy()
     from gicops_b200.search import make_c_queries
     import ctypes as C
     cq, keep = make_c_queries(qp, params)
     cp = params.c()
+    e2e_steps = min(args.steps, 5)
 
     def e2e_step():
         N.check(gx.lib().gx_search_host(dev.handle, ws.handle, C.byref(cq), C.byref(cp), out_pinned.ctypes.data,
@@ -437,23 +576,23 @@ def main():
         dist.barrier()
     if flush is None:
         t0 = time.perf_counter()
-        for _ in range(args.steps):
+        for _ in range(e2e_steps):
             e2e_step()
-        e2e_s = (time.perf_counter() - t0) / args.steps
+        e2e_s = (time.perf_counter() - t0) / e2e_steps
     else:
         e2e_s = 0.0
-        for _ in range(args.steps):
+        for _ in range(e2e_steps):
             flush.zero_()
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             e2e_step()
             e2e_s += time.perf_counter() - t0
-        e2e_s /= args.steps
+        e2e_s /= e2e_steps
     if dist:
         t = torch.tensor([e2e_s], device=d)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    h2d = q.idx.nbytes + q.moz.nbytes + q.intn.nbytes + q.prec.nbytes + 4 * q.n
+    h2d = q.idx.nbytes + q.moz.nbytes + q.intn.nbytes + q.prec.nbytes + 4 * q.n + (8 * q.n if q.dM is not None else 0)
     d2h = q.n * N.RESULT_DTYPE.itemsize + 4
 
     # ---- roofline numerator: algorithmic bytes of one launch ------------------------
@@ -472,25 +611,60 @@ def main():
         if ent:
             traffic = ent["dram_bytes_per_launch"]
 
+    # ---- parity of the benchmarked outputs (untimed) --------------------------------
+    parity = None
+    if rank == 0 and args.parity_sample and not args.plain:
+        cap = params.heap_cap
+        t_heap = torch.empty(q.n * cap * N.CELL_DTYPE.itemsize, dtype=torch.uint8, device=d)
+
+        def run_full(sel):
+            ws.search_device(qd, params, t_out.data_ptr(), t_heap.data_ptr(), t_hist.data_ptr(), stream.cuda_stream)
+            torch.cuda.synchronize()
+            ix = torch.from_numpy(sel.astype(np.int64)).to(d)
+            res_all = t_out.cpu().numpy().view(N.RESULT_DTYPE).copy()
+            hp = t_heap.view(q.n, -1).index_select(0, ix).cpu().numpy().view(N.CELL_DTYPE).reshape(len(sel), cap)
+            hs = t_hist.index_select(0, ix).cpu().numpy().view(np.uint32)
+            return res_all, hp, hs
+
+        parity = parity_block(gx, N, H, q, params, w, run_full, tail is not None, n_sample=args.parity_sample)
+        del t_heap
+    del t_hist
+
+    # ---- the plain one-spectrum-per-CTA path and the batched path on one seeded sample --
     plain = None
-    if args.compare_plain and not args.plain:
+    if args.plain_sample and not args.plain:
         import dataclasses
+        sel = np.sort(np.random.Generator(np.random.PCG64(5)).choice(q.n, size=min(q.n, args.plain_sample),
+                                                                    replace=False))
+        sq = q.subset(sel)
+        sqd, skeep = device_queries(sq)
+        s_out = torch.empty(sq.n * N.RESULT_DTYPE.itemsize, dtype=torch.uint8, device=d)
         pp = dataclasses.replace(params, flags=gx.FLAG_PLAIN)
-        ws.search_device(qd, pp, t_out.data_ptr(), stream=stream.cuda_stream)
-        torch.cuda.synchronize()
-        e0.record(stream)
-        ws.search_device(qd, pp, t_out.data_ptr(), stream=stream.cuda_stream)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        plain = {"value": q.n / (e0.elapsed_time(e1) / 1e3), "unit": unit, "steps": 1}
+
+        def timed(prm):
+            ws.search_device(sqd, prm, s_out.data_ptr(), stream=stream.cuda_stream)   # warm-up
+            torch.cuda.synchronize()
+            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a0.record(stream)
+            ws.search_device(sqd, prm, s_out.data_ptr(), stream=stream.cuda_stream)
+            a1.record(stream)
+            torch.cuda.synchronize()
+            return a0.elapsed_time(a1)
+
+        pl_ms, bt_ms = timed(pp), timed(params)
+        plain = {"value": sq.n / (pl_ms / 1e3), "unit": unit, "sample": int(sq.n), "sample_seed": 5,
+                 "batched_same_sample": sq.n / (bt_ms / 1e3), "batched_over_plain_same_sample": pl_ms / bt_ms,
+                 "batched_full_batch_over_plain": value / world / (sq.n / (pl_ms / 1e3))}
+        log(f"[bench] plain path: {plain['value']:.0f} spectra/s on {sq.n} spectra "
+            f"(batched on the same: {plain['batched_same_sample']:.0f})")
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            ref = reference_cpu(w, db, q, steps=1, warmup=1)
+            ref = reference_cpu(w, db, q, ref_sample(args.workload, q.n), steps=1, warmup=1)
             cpu = {"value": ref["value"], "unit": unit, "cores": ref["cores"], "kind": "reference",
-                   "sample": f"{ref['sample']} of {q.n} spectra, reference DSLIM_QuerySpectrum, "
-                             f"all {ref['cores']} host threads, query time only"}
+                   "sample": f"{ref['sample']} of {q.n} spectra (seeded subset, PCG64 seed 7), reference "
+                             f"DSLIM_QuerySpectrum, all {ref['cores']} host threads, query time only"}
         except Exception as ex:  # the checker binary may be absent on a machine without the reference build
             log(f"[bench] reference CPU baseline unavailable: {ex}")
 
@@ -506,9 +680,13 @@ def main():
                        "frag_tol_bins": 5, "topK": 5,
                        "l2": ("inputs larger than L2 (index %.2f GB)" % (dev.nbytes / 1e9)) if flush is None else
                              ("L2 flushed before each timed step (index %.1f MB)" % (dev.nbytes / 1e6)),
-                       "parallelism": f"replicas x{world}"},
+                       "parallelism": f"replicas x{world}",
+                       "reference_sample": f"the reference CPU path is timed on a seeded subset of "
+                                           f"{len(ref_sample(args.workload, q.n))} of these {q.n} spectra (PCG64 "
+                                           "seed 7; its whole batch would take minutes per step); the subset is a "
+                                           "uniform draw from the same batch"},
             "e2e": {"value": q.n * world / e2e_s, "unit": unit, "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h)},
+                    "d2h_bytes_per_step": int(d2h), "steps": e2e_steps},
             "roofline": {"bound": "hbm", "kernel": top_k, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "algorithmic_bytes_per_launch": bytes_launch, "kernel_ms": k_ms,
@@ -516,6 +694,7 @@ def main():
             "kernel_ms": {k: v[1] / v[0] for k, v in kt.items()},
             "gpu_launches": launches,
             "path": "plain" if args.plain else ("batched+learned tail" if tail else "batched"),
+            "parity": parity,
             "index_build": index_build,
             "prep": prep,
             "learned_tail": dict(tail_info or {}, queries_replaced=int(

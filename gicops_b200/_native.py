@@ -30,6 +30,7 @@ STATUS_NAMES = {
 FLAG_WIDE_SCORECARD = 1
 FLAG_PLAIN = 2
 STATUS_LEARNED_TAIL = 16
+STATUS_PEAK_LIMIT = 32
 
 TAIL_WINDOW = 128
 TAIL_IN = 132
@@ -160,6 +161,7 @@ _SIGS = [
     ("gx_tail_apply", C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                   C.c_uint32, C.c_double, C.c_void_p]),
     ("gx_tail_check", C.c_int32, [C.c_void_p]),
+    ("gx_tail_set_wait_limit", C.c_int32, [C.c_uint64]),
     ("gx_workspace_set_tail", C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32]),
     ("gx_tail_gemm", C.c_int32, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_int64, C.c_int64, C.c_int32,
                                  C.c_int32, C.c_int32, C.c_void_p, C.c_int64, C.c_void_p]),

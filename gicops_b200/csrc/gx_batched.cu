@@ -30,6 +30,9 @@ namespace gx {
 // k_prep: one CTA per spectrum
 // ------------------------------------------------------------------------------------
 constexpr int kPrepBlock = 256;
+// guard word of a spectrum k_prep rejects (more than GX_MAX_PEAKS peaks, or more intervals
+// than the workspace holds); 0 and 1 say whether the packed scorecard is exact
+constexpr uint32_t kGuardRejected = 2u;
 
 __global__ void __launch_bounds__(kPrepBlock) k_prep(SearchArgs a, int2 *win, uint64_t *work_key, uint32_t *order0)
 {
@@ -49,7 +52,7 @@ __global__ void __launch_bounds__(kPrepBlock) k_prep(SearchArgs a, int2 *win, ui
         if (tid == 0) {
             atomicExch(a.err, 1);
             a.nivl[s] = 0;
-            a.guard[s] = 1;
+            a.guard[s] = kGuardRejected;   // k_search_batched writes the spectrum's flagged empty row
             work_key[s] = 0;
             order0[s] = s;
         }
@@ -659,15 +662,9 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
         __syncthreads();
         const int s = sm.spec;
         if (s < 0) break;
-        if (a.nivl[s] == 0) {                 // no probed bins, or flagged by k_prep
-            if (tid == 0) {
-                gx_result r;
-                memset(&r, 0, sizeof(r));
-                a.out[s] = r;
-            }
-            for (int i = tid; i < kHist; i += kBBlock) a.hist_g[(uint64_t)s * kHist + i] = 0;
-            if (a.heap_out)
-                for (int i = tid; i < a.heap_cap; i += kBBlock) a.heap_out[(uint64_t)s * a.heap_cap + i] = gx_cell{};
+        if (a.nivl[s] == 0) {                 // no probed bins, or rejected by k_prep
+            write_empty_row(a, a.hist_g, (uint32_t)s, a.guard[s] == kGuardRejected ? GX_STATUS_PEAK_LIMIT : 0, tid,
+                            kBBlock);
             continue;
         }
         const bool wide = a.guard[s] == 0 || (a.flags & GX_FLAG_WIDE_SCORECARD);

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cstring>
 
 #include "../../include/gicops_b200.h"
 
@@ -89,7 +90,8 @@ struct SearchArgs {
     Interval *ivl;        // [2 * npeaks]: intervals of spectrum s start at 2 * qidx[s]
     uint64_t ivl_cap;     // intervals the buffer holds
     uint32_t *nivl;       // [nspec]
-    uint32_t *guard;      // [nspec]: 1 if the packed scorecard is exact for the spectrum
+    uint32_t *guard;      // [nspec]: 1 if the packed scorecard is exact for the spectrum, 0 if not,
+                          // 2 if the spectrum was rejected (not searched)
     const uint32_t *order;// [nspec] spectra, heaviest first
     uint32_t *queue;      // work-queue head
     uint32_t *hist_g;     // [nspec * kHist] histograms (always)
@@ -136,6 +138,24 @@ __device__ __forceinline__ void heap_insert(Cell *a, int &size, int cap, const C
 __device__ __forceinline__ bool fits_tail(int32_t cpsms, uint32_t min_cpsm)
 {
     return cpsms > 0 && (uint32_t)cpsms >= min_cpsm;
+}
+
+// The outputs of spectrum s when it is not searched (no probed bin, or a spectrum the
+// device guard rejected): a zeroed result record with `status`, an empty histogram row
+// and an empty heap row.  Called by every thread of the block (nthreads of them).
+__device__ __forceinline__ void write_empty_row(const SearchArgs &a, uint32_t *hist, uint32_t s, int32_t status,
+                                                int tid, int nthreads)
+{
+    if (tid == 0) {
+        gx_result r;
+        memset(&r, 0, sizeof(r));
+        r.status = status;
+        a.out[s] = r;
+    }
+    if (hist)
+        for (int i = tid; i < kHist; i += nthreads) hist[(uint64_t)s * kHist + i] = 0u;
+    if (a.heap_out)
+        for (int i = tid; i < a.heap_cap; i += nthreads) a.heap_out[(uint64_t)s * a.heap_cap + i] = gx_cell{};
 }
 
 __device__ __forceinline__ Cell heap_getmax(const Cell *a, int size)

@@ -24,6 +24,7 @@
 #include "../../include/gicops_b200.h"
 #include "gx_device.cuh"
 #include "gx_index.cuh"
+#include "gx_device_scope.cuh"
 #include "gx_internal.h"
 #include "gx_ions.h"
 
@@ -94,7 +95,7 @@ using namespace gx;
 extern "C" gx_status gx_index_free(gx_index *ix)
 {
     if (!ix) return GX_SUCCESS;
-    cudaSetDevice(ix->device);
+    DeviceScope ds(ix->device);
     cudaFree(ix->bA);
     cudaFree(ix->iA);
     cudaFree(ix->iAb);
@@ -235,6 +236,7 @@ extern "C" gx_status gx_index_upload(const gx_length_desc *lens, int32_t nlen, u
     gx_index *ix = nullptr;
     void *scan_tmp = nullptr;
     size_t scan_bytes = 0;
+    DeviceScope ds(device);   // the caller's device is current again on return
     gx_status st = alloc_index(hl, nlen, nbins, maxz, tot_ia, tot_m, tot_blk, device, &ix, &scan_tmp, &scan_bytes,
                                "gx_index_upload");
     if (st != GX_SUCCESS) return st;
@@ -370,6 +372,7 @@ extern "C" gx_status gx_index_build(gx_host_length *const *lens, int32_t nlen, c
     gx_index *ix = nullptr;
     void *scan_tmp = nullptr;
     size_t scan_bytes = 0;
+    DeviceScope ds(device);   // the caller's device is current again on return
     gx_status st = alloc_index(hl, nlen, nbins, bp->maxz, tot_ia, tot_m, tot_blk, device, &ix, &scan_tmp, &scan_bytes,
                                "gx_index_build");
     if (st != GX_SUCCESS) return st;
@@ -447,7 +450,8 @@ extern "C" gx_status gx_index_read_length(const gx_index *ix, int32_t i, uint32_
 {
     if (!ix) return fail(GX_ERR_INVLD_PTR, "gx_index_read_length: null index");
     if (i < 0 || i >= ix->nlen) return fail(GX_ERR_INVLD_PARAM, "gx_index_read_length: no such length");
-    cudaError_t e = cudaSetDevice(ix->device);
+    DeviceScope ds(ix->device);
+    cudaError_t e = ds.status();
     if (e != cudaSuccess) return cuda_fail(e, "gx_index_read_length: cudaSetDevice");
     const DevLen &l = ix->hlens[i];
     const uint64_t n = (uint64_t)l.npep * l.speclen;

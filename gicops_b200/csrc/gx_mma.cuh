@@ -72,11 +72,24 @@ __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
 }
 
-// Bounded wait for phase `parity` of `bar`; false when the bound ran out.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t max_tries)
+// Nanoseconds of the GPU's global timer.
+__device__ __forceinline__ uint64_t global_ns()
 {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Waits for phase `parity` of `bar` for at most `budget_ns` nanoseconds of the global
+// timer; false when the budget ran out (a budget of 0 gives up without looking).  Each
+// try_wait may suspend the thread for a system-dependent interval, so the timer is read
+// between attempts: the bound is time, not a count of attempts.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint64_t budget_ns)
+{
+    if (budget_ns == 0) return false;
     const uint32_t a = smem_addr(bar);
-    for (uint32_t i = 0; i < max_tries; i++) {
+    const uint64_t t0 = global_ns();
+    for (;;) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -86,8 +99,8 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32
             : "r"(a), "r"(parity)
             : "memory");
         if (done) return true;
+        if (global_ns() - t0 >= budget_ns) return false;
     }
-    return false;
 }
 
 __device__ __forceinline__ void fence_smem_to_async()

@@ -12,7 +12,8 @@
 // and the device guard word.  It is a static __device__ array, so in host code its name
 // is only a host-side stand-in: the kernels receive the device address that
 // cudaGetSymbolAddress returns, looked up once per device (with that device current) on
-// the first call that runs on it.
+// the first call that runs on it, and again after a cudaDeviceReset has replaced the
+// device's context (the new context holds a fresh, zeroed copy of the array).
 //
 // Limits and sharing:
 //  * at most GX_NOALLOC_MAX_WINDOWS (spectra x lengths) per call;
@@ -30,6 +31,7 @@
 
 #include "../../include/gicops_b200.h"
 #include "gx_device.cuh"
+#include "gx_device_scope.cuh"
 #include "gx_index.cuh"
 #include "gx_internal.h"
 
@@ -52,14 +54,47 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
-unsigned char *g_scratch_dev[kMaxDevices] = {};
+struct DeviceSetUp {
+    unsigned char *addr = nullptr;   // the array's device address in that context
+    unsigned long long ctx_id = 0;   // the context it was set up in (0: never)
+};
+DeviceSetUp g_setup[kMaxDevices];
 
-// Device address of the scratch array on `device` (current device), set up on first use.
+// Unique id of the calling thread's current context (0 when none or when the driver has no
+// such query).  A cudaDeviceReset replaces the device's primary context, and with it the
+// module's copy of the array: a new id says that the set-up must run again.
+unsigned long long current_context_id()
+{
+    using GetCurrent = int (*)(void **);
+    using GetId = int (*)(void *, unsigned long long *);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static bool looked_up = false;
+    if (!looked_up) {   // under g_mu
+        void *f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault) == cudaSuccess)
+            get_current = reinterpret_cast<GetCurrent>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault) == cudaSuccess)
+            get_id = reinterpret_cast<GetId>(f);
+        cudaGetLastError();
+        looked_up = true;
+    }
+    void *ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+    return id;
+}
+
+// Device address of the scratch array on `device` (the current device), set up on the
+// first call in each context: the address is looked up and the hyperscore table written.
 gx_status scratch_for(int device, unsigned char **out)
 {
     if (device < 0 || device >= kMaxDevices) return fail(GX_ERR_INVLD_PARAM, "gx_search_device_noalloc: device id");
     std::lock_guard<std::mutex> g(g_mu);
-    if (!g_scratch_dev[device]) {
+    DeviceSetUp &d = g_setup[device];
+    const unsigned long long ctx = current_context_id();
+    if (!d.addr || ctx == 0 || ctx != d.ctx_id) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) return cuda_fail(e, "gx_search_device_noalloc: cudaGetSymbolAddress");
@@ -70,9 +105,10 @@ gx_status scratch_for(int device, unsigned char **out)
         if ((e = cudaFuncSetAttribute(k_search_plain, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       kPlainTile * 8)) != cudaSuccess)
             return cuda_fail(e, "gx_search_device_noalloc: kernel attributes");
-        g_scratch_dev[device] = static_cast<unsigned char *>(p);
+        d.addr = static_cast<unsigned char *>(p);
+        d.ctx_id = current_context_id();   // the lookup above made the context current
     }
-    *out = g_scratch_dev[device];
+    *out = d.addr;
     return GX_SUCCESS;
 }
 
@@ -98,8 +134,10 @@ extern "C" gx_status gx_search_device_noalloc(gx_index *ix, const gx_queries *q,
                                            " exceeds the fixed scratch of " +
                                            std::to_string(GX_NOALLOC_MAX_WINDOWS) + " windows; split the batch");
     if (q->nspec == 0) return GX_SUCCESS;
-    cudaError_t e = cudaSetDevice(ix->device);
+    DeviceScope ds(ix->device);
+    cudaError_t e = ds.status();
     if (e != cudaSuccess) return cuda_fail(e, "gx_search_device_noalloc: cudaSetDevice");
+    cudaGetLastError();   // an earlier call's error is not ours to report
     unsigned char *scratch = nullptr;
     gx_status rc = scratch_for(ix->device, &scratch);
     if (rc != GX_SUCCESS) return rc;

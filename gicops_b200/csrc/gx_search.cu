@@ -19,6 +19,7 @@
 
 #include "../../include/gicops_b200.h"
 #include "gx_batched.h"
+#include "gx_device_scope.cuh"
 #include "gx_index.cuh"
 #include "gx_device.cuh"
 #include "gx_internal.h"
@@ -186,8 +187,9 @@ __global__ void __launch_bounds__(kBlock) k_search_plain(SearchArgs a, int tile)
     for (int i = tid; i < 81; i += kBlock) sm.lgf[i] = a.lgfact[i];
     __syncthreads();
     const uint32_t q0 = a.qidx[s], q1 = a.qidx[s + 1];
-    if (q1 - q0 > GX_MAX_PEAKS) {
+    if (q1 < q0 || q1 - q0 > GX_MAX_PEAKS) {   // not searched: a defined row, flagged
         if (tid == 0) atomicExch(a.err, 1);
+        write_empty_row(a, a.hist_out, s, GX_STATUS_PEAK_LIMIT, tid, kBlock);
         return;
     }
     unsigned long long sum_in = 0;
@@ -454,7 +456,7 @@ extern "C" int32_t gx_heap_capacity(uint32_t topmatches)
 extern "C" gx_status gx_workspace_free(gx_workspace *ws)
 {
     if (!ws) return GX_SUCCESS;
-    cudaSetDevice(ws->device);
+    DeviceScope ds(ws->device);
     void *ptrs[] = {ws->win, ws->lgfact, ws->err, ws->qidx, ws->moz, ws->intn, ws->charge, ws->prec,
                     ws->dMq, ws->out, ws->heap, ws->hist, ws->ivl, ws->nivl, ws->guard, ws->queue,
                     ws->hist_g, ws->spill, ws->logtab, ws->bs.key_in, ws->bs.key_out, ws->bs.ord_in, ws->bs.ord_out, ws->bs.sort_temp};
@@ -471,7 +473,8 @@ extern "C" gx_status gx_workspace_create(const gx_index *ix, uint32_t max_spec, 
     if (!ix || !out) return fail(GX_ERR_INVLD_PTR, "gx_workspace_create: null argument");
     *out = nullptr;
     if (max_spec == 0) return fail(GX_ERR_INVLD_PARAM, "gx_workspace_create: max_spec must be > 0");
-    GX_CUDA(cudaSetDevice(ix->device));
+    DeviceScope ds(ix->device);
+    GX_CUDA(ds.status());
     auto *ws = new gx_workspace();
     ws->ix = ix;
     ws->device = ix->device;
@@ -624,7 +627,8 @@ extern "C" gx_status gx_search_device(gx_index *ix, gx_workspace *ws, const gx_q
 {
     if (!ix || !ws || !q || !p || !out) return fail(GX_ERR_INVLD_PTR, "gx_search_device: null argument");
     if (ws->ix != ix) return fail(GX_ERR_INVLD_PARAM, "gx_search_device: workspace belongs to another index");
-    GX_CUDA(cudaSetDevice(ix->device));
+    DeviceScope ds(ix->device);
+    GX_CUDA(ds.status());
     return launch_search(ix, ws, q, p, out, heap, hist, (cudaStream_t)stream);
 }
 
@@ -641,7 +645,8 @@ extern "C" gx_status gx_search_host(gx_index *ix, gx_workspace *ws, const gx_que
     int32_t cap;
     gx_status rc = check_params(ix, p, &cap);
     if (rc != GX_SUCCESS) return rc;
-    GX_CUDA(cudaSetDevice(ix->device));
+    DeviceScope ds(ix->device);
+    GX_CUDA(ds.status());
     cudaStream_t st = ws->stream;
     const uint32_t n = q->nspec;
     if (heap_out && !ws->heap) GX_CUDA(cudaMalloc(&ws->heap, sizeof(gx_cell) * GX_MAX_HEAP * (uint64_t)ws->max_spec));

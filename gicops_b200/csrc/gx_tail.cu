@@ -25,6 +25,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -34,6 +35,7 @@
 
 #include "../../include/gicops_b200.h"
 #include "gx_device.cuh"
+#include "gx_device_scope.cuh"
 #include "gx_internal.h"
 #include "gx_mma.cuh"
 
@@ -239,12 +241,15 @@ struct GemmArgs {
     const float *Z;       // kEpiDGelu: pre-activation of the forward pass
     long long ldz;
     int32_t *err;
+    uint64_t wait_ns;     // limit of each wait for the tensor core (global-timer nanoseconds)
 };
 
 constexpr int kGemmThreads = 128;
 constexpr int kKStage = 64;
 constexpr int kATileBytes = 128 * kKStage * 2;
-constexpr long long kWaitCycles = 4000000000ll;   // about two seconds
+// After a wait has given up, the kernel still waits this long for the MMA it issued last
+// (it reads the operand tiles and writes the TMEM that the kernel frees afterwards).
+constexpr uint64_t kDrainNs = 1000000000ull;
 
 __device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
 __device__ __forceinline__ float gelu_grad(float z)
@@ -356,7 +361,7 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(GemmArgs a)
             mma::mma_commit(&bar);
         }
         // the tiles are restaged next round: wait for the tensor core to finish reading
-        ok = mma::mbar_wait(&bar, phase, kWaitCycles);
+        ok = mma::mbar_wait(&bar, phase, a.wait_ns);
         phase ^= 1u;
         if (__syncthreads_or(!ok)) {   // uniform: the warp-wide TMEM loads below need it
             ok = false;
@@ -365,7 +370,7 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(GemmArgs a)
     }
     if (!ok) {
         if (tid == 0 && a.err) atomicExch(a.err, 2);
-        mma::mbar_wait(&bar, phase ^ 1u, kWaitCycles);   // the outstanding commit, bounded
+        mma::mbar_wait(&bar, phase ^ 1u, kDrainNs);   // the outstanding commit, bounded
     } else {
         mma::fence_after_sync();
         const int row = m0 + warp * 32 + lane;
@@ -502,6 +507,9 @@ namespace {
 
 std::mutex g_attr_mu;
 bool g_attr_done[64] = {};
+// limit of each tensor-core wait of k_gemm (gx_tail_set_wait_limit)
+constexpr uint64_t kDefaultWaitNs = 1000000000ull;
+std::atomic<uint64_t> g_wait_ns{kDefaultWaitNs};
 
 // Dynamic shared memory of every k_gemm CTA.  The operand tiles need at most 48 KB; the
 // request is padded so that at most two CTAs share an SM, whose 512 TMEM columns then
@@ -542,7 +550,8 @@ gx_status gemm(const gx_tail_model *m, const bf16 *A, long long sam, long long s
                const float *bias, const float *Z, long long ldz, cudaStream_t st)
 {
     if (M <= 0 || N <= 0 || K <= 0) return fail(GX_ERR_INVLD_SIZE, "tail model: empty GEMM");
-    GemmArgs a{A, sam, sak, B, sbn, sbk, M, N, K, ntile(N), epi, D, ldd, H, ldh, bias, Z, ldz, m ? m->err : nullptr};
+    GemmArgs a{A,   sam, sak, B,    sbn, sbk, M, N, K, ntile(N), epi, D, ldd, H, ldh, bias, Z, ldz,
+               m ? m->err : nullptr, g_wait_ns.load(std::memory_order_relaxed)};
     dim3 grid((unsigned)((M + 127) / 128), (unsigned)((N + a.NT - 1) / a.NT));
     int h = prof_begin("k_gemm", st);
     k_gemm<<<grid, kGemmThreads, kGemmSmem, st>>>(a);
@@ -615,9 +624,15 @@ gx_status check_model(const gx_tail_model *m, uint32_t n, const char *what)
     if (n > m->max_batch)
         return fail(GX_ERR_INVLD_SIZE, std::string(what) + ": batch of " + std::to_string(n) + " rows exceeds max_batch " +
                                            std::to_string(m->max_batch));
-    cudaError_t e = cudaSetDevice(m->device);
-    return e == cudaSuccess ? GX_SUCCESS : cuda_fail(e, what);
+    return GX_SUCCESS;
 }
+
+// Checks the model and batch, then makes the model's device current for the rest of the
+// calling entry point (the caller's device is current again when it returns).
+#define GX_MODEL_SCOPE(m, n, what)                                              \
+    GX_TRY(check_model(m, n, what));                                            \
+    DeviceScope model_scope_((m)->device);                                      \
+    if (model_scope_.status() != cudaSuccess) return cuda_fail(model_scope_.status(), what)
 
 }  // namespace
 
@@ -631,7 +646,8 @@ extern "C" gx_status gx_tail_model_create(int32_t device, uint32_t max_batch, ui
     *out = nullptr;
     if (max_batch == 0 || max_batch > (1u << 22))
         return fail(GX_ERR_INVLD_SIZE, "gx_tail_model_create: max_batch must be in 1..2^22");
-    cudaError_t e = cudaSetDevice(device);
+    DeviceScope ds(device);
+    cudaError_t e = ds.status();
     if (e != cudaSuccess) return cuda_fail(e, "gx_tail_model_create: cudaSetDevice");
     GX_TRY(set_attributes(device));
     gx_tail_model *m = new gx_tail_model;
@@ -676,7 +692,7 @@ extern "C" gx_status gx_tail_model_create(int32_t device, uint32_t max_batch, ui
 extern "C" gx_status gx_tail_model_free(gx_tail_model *m)
 {
     if (!m) return GX_SUCCESS;
-    cudaSetDevice(m->device);
+    DeviceScope ds(m->device);
     for (void *p : m->allocs) cudaFree(p);
     delete m;
     return GX_SUCCESS;
@@ -684,7 +700,7 @@ extern "C" gx_status gx_tail_model_free(gx_tail_model *m)
 
 extern "C" gx_status gx_tail_model_set(gx_tail_model *m, const float *params, const float *norm)
 {
-    GX_TRY(check_model(m, 0, "gx_tail_model_set"));
+    GX_MODEL_SCOPE(m, 0, "gx_tail_model_set");
     cudaError_t e;
     if (params) {
         if ((e = cudaMemcpy(m->P, params, kNParam * sizeof(float), cudaMemcpyHostToDevice)) != cudaSuccess)
@@ -709,7 +725,7 @@ extern "C" gx_status gx_tail_model_set(gx_tail_model *m, const float *params, co
 
 extern "C" gx_status gx_tail_model_get(const gx_tail_model *m, float *params, float *norm, uint64_t *steps)
 {
-    GX_TRY(check_model(m, 0, "gx_tail_model_get"));
+    GX_MODEL_SCOPE(m, 0, "gx_tail_model_get");
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return cuda_fail(e, "gx_tail_model_get");
     if (params && (e = cudaMemcpy(params, m->P, kNParam * sizeof(float), cudaMemcpyDeviceToHost)) != cudaSuccess)
@@ -724,7 +740,7 @@ extern "C" gx_status gx_tail_features(gx_tail_model *m, const uint32_t *hist_dev
                                       const gx_tail_sample *samples_host, uint32_t n, uint16_t *x_dev,
                                       uint32_t *sub_hist_dev, int32_t *sub_cpsms_dev, int32_t *hyp_dev, void *stream)
 {
-    GX_TRY(check_model(m, n, "gx_tail_features"));
+    GX_MODEL_SCOPE(m, n, "gx_tail_features");
     if (n == 0) return GX_SUCCESS;
     if (!hist_dev || !res_dev || !prec_dev || !samples_host || !x_dev)
         return fail(GX_ERR_INVLD_PTR, "gx_tail_features: null argument");
@@ -765,7 +781,7 @@ extern "C" gx_status gx_tail_fit_rows(const uint32_t *hist_dev, const int32_t *c
 extern "C" gx_status gx_tail_grad(gx_tail_model *m, const uint16_t *x_dev, const float *target_dev, uint32_t n,
                                   const float *weights2, float *grad_dev, float *loss_dev, void *stream)
 {
-    GX_TRY(check_model(m, n, "gx_tail_grad"));
+    GX_MODEL_SCOPE(m, n, "gx_tail_grad");
     if (n == 0 || !x_dev || !target_dev) return fail(GX_ERR_INVLD_PARAM, "gx_tail_grad: empty batch or null input");
     cudaStream_t st = (cudaStream_t)stream;
     cudaError_t e = cudaMemsetAsync(m->loss, 0, sizeof(float), st);
@@ -783,7 +799,7 @@ extern "C" gx_status gx_tail_grad(gx_tail_model *m, const uint16_t *x_dev, const
 extern "C" gx_status gx_tail_train_step(gx_tail_model *m, const uint16_t *x_dev, const float *target_dev, uint32_t n,
                                         const gx_tail_adam *opt, float *loss_dev, void *stream)
 {
-    GX_TRY(check_model(m, n, "gx_tail_train_step"));
+    GX_MODEL_SCOPE(m, n, "gx_tail_train_step");
     if (n == 0 || !x_dev || !target_dev || !opt)
         return fail(GX_ERR_INVLD_PARAM, "gx_tail_train_step: empty batch or null input");
     cudaStream_t st = (cudaStream_t)stream;
@@ -805,7 +821,7 @@ extern "C" gx_status gx_tail_train_step(gx_tail_model *m, const uint16_t *x_dev,
 
 extern "C" gx_status gx_tail_predict(gx_tail_model *m, const uint16_t *x_dev, uint32_t n, float *pred_dev, void *stream)
 {
-    GX_TRY(check_model(m, n, "gx_tail_predict"));
+    GX_MODEL_SCOPE(m, n, "gx_tail_predict");
     if (n == 0) return GX_SUCCESS;
     if (!x_dev || !pred_dev) return fail(GX_ERR_INVLD_PTR, "gx_tail_predict: null argument");
     cudaStream_t st = (cudaStream_t)stream;
@@ -818,7 +834,7 @@ extern "C" gx_status gx_tail_apply(gx_tail_model *m, const uint32_t *hist_dev, g
                                    const float *prec_dev, const int32_t *charge_dev, uint32_t nspec,
                                    uint32_t sparse_below, double expect_max, void *stream)
 {
-    GX_TRY(check_model(m, 0, "gx_tail_apply"));
+    GX_MODEL_SCOPE(m, 0, "gx_tail_apply");
     if (nspec == 0 || sparse_below == 0) return GX_SUCCESS;
     if (!hist_dev || !res_dev || !prec_dev) return fail(GX_ERR_INVLD_PTR, "gx_tail_apply: null argument");
     cudaStream_t st = (cudaStream_t)stream;
@@ -844,12 +860,19 @@ extern "C" gx_status gx_tail_apply(gx_tail_model *m, const uint32_t *hist_dev, g
 
 extern "C" gx_status gx_tail_check(gx_tail_model *m)
 {
-    GX_TRY(check_model(m, 0, "gx_tail_check"));
+    GX_MODEL_SCOPE(m, 0, "gx_tail_check");
     int32_t v = 0;
     cudaError_t e = cudaMemcpy(&v, m->err, sizeof(v), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_fail(e, "gx_tail_check");
+    if (v == 0) return GX_SUCCESS;
+    if ((e = cudaMemset(m->err, 0, sizeof(int32_t))) != cudaSuccess) return cuda_fail(e, "gx_tail_check: clear");
     if (v == 1) return fail(GX_ERR_DEVICE_GUARD, "tail model: a sample had an invalid top bin");
-    if (v == 2) return fail(GX_ERR_DEVICE_GUARD, "tail model: a tensor-core wait ran out");
+    return fail(GX_ERR_DEVICE_GUARD, "tail model: a tensor-core wait ran out");
+}
+
+extern "C" gx_status gx_tail_set_wait_limit(uint64_t ns)
+{
+    g_wait_ns.store(ns, std::memory_order_relaxed);
     return GX_SUCCESS;
 }
 

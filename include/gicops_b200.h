@@ -210,7 +210,10 @@ typedef struct {
 /* Per-spectrum result.  status bits: 1 = cpsms >= max(min_cpsm, 1) (e-value computed),
  * 2 = e_x < expect_max (a PSM the reference prints), 4 = a shared-ion count above
  * MAX_SHDPEAKS (80) was clamped, 8 = the 12-byte scorecard was used, 16 = the e-value
- * comes from the learned tail (gx_tail_apply). */
+ * comes from the learned tail (gx_tail_apply), 32 = GX_STATUS_PEAK_LIMIT: the spectrum has
+ * more than GX_MAX_PEAKS peaks and was not searched (every other field zero, its histogram
+ * and heap rows empty; gx_search_host also returns GX_ERR_DEVICE_GUARD for the batch). */
+#define GX_STATUS_PEAK_LIMIT 32
 typedef struct {
     int32_t cpsms;
     int32_t status;
@@ -265,8 +268,10 @@ gx_status gx_search_device(gx_index *ix, gx_workspace *ws, const gx_queries *q_d
  * exit); batches with nspec * nlen above that are rejected with GX_ERR_INVLD_SIZE.  The
  * first call on a device looks the array up and sets the kernel up on that device: make
  * it before any stream capture.  All calls share the array; calls that overlap on the GPU
- * race and must be serialised by the caller.  Stream-ordered, no synchronisation; the
- * device guard word (too many peaks) is not reported. */
+ * race and must be serialised by the caller.  Stream-ordered, no synchronisation: a
+ * spectrum over GX_MAX_PEAKS peaks is reported through its status (GX_STATUS_PEAK_LIMIT).
+ * A cudaDeviceReset (or release of the primary context) drops the array's contents; the
+ * next call on that device notices the new context and sets the array up again. */
 #define GX_NOALLOC_MAX_WINDOWS (1u << 19)
 gx_status gx_search_device_noalloc(gx_index *ix, const gx_queries *q_dev, const gx_params *p, gx_result *out_dev,
                                    gx_cell *heap_dev, uint32_t *hist_dev, void *stream);
@@ -378,8 +383,16 @@ gx_status gx_tail_apply(gx_tail_model *m, const uint32_t *hist_dev, gx_result *r
  * gx_tail_apply with sparse_below after the plain fit, on the workspace's stream or the
  * caller's.  The model must live on the index's device and outlive the attachment. */
 gx_status gx_workspace_set_tail(gx_workspace *ws, gx_tail_model *m, uint32_t sparse_below);
-/* Synchronises and reports a device-side guard of the model's kernels. */
+/* Synchronises, reports a device-side guard of the model's kernels (GX_ERR_DEVICE_GUARD)
+ * and clears it, so that the next check reports only what came after this one. */
 gx_status gx_tail_check(gx_tail_model *m);
+/* Time limit of each wait of the model's tensor-core kernel for its matrix products, in
+ * nanoseconds of the GPU clock (default 1,000,000,000, one second; applies to launches made
+ * after the call, process-wide).  A wait that runs out makes the kernel record the guard
+ * that gx_tail_check reports, wait (at most one more second) for the product it issued
+ * last, free its tensor memory and return without writing its output.  0 makes every
+ * wait give up at once: a way to exercise that path.  No counterpart in the reference. */
+gx_status gx_tail_set_wait_limit(uint64_t ns);
 /* The model's tensor-core GEMM alone: D[M][N] (fp32, row stride ldd) = A * B^T with
  * A(m,k) = a[m*sam + k*sak], B(n,k) = b[n*sbn + k*sbk] (bf16 bits), on the current device. */
 gx_status gx_tail_gemm(const uint16_t *a_dev, int64_t sam, int64_t sak, const uint16_t *b_dev, int64_t sbn,

@@ -18,8 +18,10 @@
 //               [--mods M:15.9949:2 ...] [--nmods 2] [--threads N] [--topmatches 5]
 //               [--expect-max 1e300] [--queries Q.pbin] [--first N] [--repeat R]
 //               [--out RES.bin] [--dump-index IDX.bin] [--qdm DM.f64]
-//               [--min-cpsm 4] [--min-shp 4]
+//               [--min-cpsm 4] [--min-shp 4] [--entries-only]
 //   ref_harness --ms2-to-pbin FILE.ms2     (the reference's MS2 conversion: FILE.ms2.pbin)
+// --entries-only stops after the index entries (LBE_* steps, no fragment-ion index) and,
+// with --dump-index, writes them alone (magic GXREFEN1: no bA / iA arrays).
 // --qdm gives one precursor tolerance (Da, float64) per spectrum: each spectrum is then
 // searched alone with params.dM set to its value (the reference reads params.dM at
 // call time in DSLIM_BinarySearch, source/core/dslim_query.cpp:1102-1106).
@@ -140,6 +142,7 @@ int main(int argc, char **argv)
     int topmatches = 5, first = -1, repeat = 1, min_cpsm = 4, min_shp = 4;
     double dM = 10.0, expect_max = 1e300;
     unsigned dF = 5;
+    bool entries_only = false;
 
     for (int i = 1; i < argc; i++) {
         std::string a = argv[i];
@@ -167,6 +170,7 @@ int main(int argc, char **argv)
         else if (a == "--min-cpsm") min_cpsm = std::atoi(nxt().c_str());
         else if (a == "--min-shp") min_shp = std::atoi(nxt().c_str());
         else if (a == "--ms2-to-pbin") ms2path = nxt();
+        else if (a == "--entries-only") entries_only = true;
         else { std::fprintf(stderr, "unknown option %s\n", a.c_str()); return 2; }
     }
     if (!ms2path.empty()) {
@@ -243,10 +247,10 @@ int main(int argc, char **argv)
             std::fprintf(stderr, "length %d split into %u chunks\n", L, ix->nChunks);
             st = ERR_INVLD_SIZE;
         }
-        if (st == SLM_SUCCESS) st = DSLIM_Construct(ix);
+        if (st == SLM_SUCCESS && !entries_only) st = DSLIM_Construct(ix);
     }
-    if (st == SLM_SUCCESS) st = DSLIM_DeallocateSpecArr();
-    if (st == SLM_SUCCESS) st = DSLIM_InitializeScorecard(index, nlen);
+    if (st == SLM_SUCCESS && !entries_only) st = DSLIM_DeallocateSpecArr();
+    if (st == SLM_SUCCESS && !entries_only) st = DSLIM_InitializeScorecard(index, nlen);
     double t1 = now_s();
     if (st != SLM_SUCCESS) { std::fprintf(stderr, "index build failed: %d\n", st); return 1; }
 
@@ -254,7 +258,7 @@ int main(int argc, char **argv)
         FILE *f = std::fopen(dumppath.c_str(), "wb");
         if (!f) { std::perror("dump"); return 1; }
         const uint32_t nb = (uint32_t)(params.max_mass * params.scale) + 1;
-        std::fwrite("GXREFIX1", 1, 8, f);
+        std::fwrite(entries_only ? "GXREFEN1" : "GXREFIX1", 1, 8, f);
         int32_t hdr[4] = {nlen, minlen, maxz, (int32_t)nb};
         std::fwrite(hdr, 4, 4, f);
         for (int i = 0; i < nlen; i++) {
@@ -268,6 +272,7 @@ int main(int argc, char **argv)
             for (uint32_t k = 0; k < N; k++) std::fwrite(&ix->pepEntries[k].seqID, 4, 1, f);
             for (uint32_t k = 0; k < N; k++) std::fwrite(&ix->pepEntries[k].sites.sites, 8, 1, f);
             for (uint32_t k = 0; k < N; k++) std::fwrite(&ix->pepEntries[k].sites.modNum, 4, 1, f);
+            if (entries_only) continue;
             std::fwrite(ix->ionIndex[0].bA, 4, nb, f);
             std::fwrite(ix->ionIndex[0].iA, 4, (size_t)N * speclen, f);
         }
@@ -277,7 +282,7 @@ int main(int argc, char **argv)
     double tq = 0.0;
     std::vector<double> t_each;
     size_t nspec = 0;
-    if (!qpath.empty()) {
+    if (!qpath.empty() && !entries_only) {
         std::vector<Spec> specs;
         if (!read_pbin(qpath, specs)) { std::fprintf(stderr, "bad pbin %s\n", qpath.c_str()); return 1; }
         if (first >= 0 && (size_t)first < specs.size()) specs.resize(first);

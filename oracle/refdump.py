@@ -3,7 +3,7 @@
 
 * index dump (``--dump-index``): per length L the peptide sequences, the index
   entries in the reference's final (mass-sorted) order, and the CSR arrays bA/iA
-  built by source/core/dslim.cpp:46-153;
+  built by source/core/dslim.cpp:46-153 (left out with ``--entries-only``);
 * PSM capture (``--out``): one 32-byte record per spectrum with the fields that
   source/core/dslim_query.cpp:1017-1061 hands to DFile_PrintScore.
 """
@@ -23,9 +23,12 @@ def read_capture(path: str) -> np.ndarray:
 
 
 def read_index_dump(path: str):
-    """Returns (header dict, list of per-length dicts)."""
+    """Returns (header dict, list of per-length dicts).  An entries-only dump
+    (``--entries-only``, magic GXREFEN1) has no bA / iA arrays."""
     raw = np.fromfile(path, dtype=np.uint8)
-    assert raw[:8].tobytes() == b"GXREFIX1", "not a reference index dump"
+    magic = raw[:8].tobytes()
+    assert magic in (b"GXREFIX1", b"GXREFEN1"), "not a reference index dump"
+    full = magic == b"GXREFIX1"
     off = 8
     nlen, minlen, maxz, nb = np.frombuffer(raw, dtype="<i4", count=4, offset=off)
     off += 16
@@ -39,8 +42,10 @@ def read_index_dump(path: str):
         seqid = np.frombuffer(raw, dtype="<u4", count=N, offset=off).copy(); off += 4 * N
         sites = np.frombuffer(raw, dtype="<u8", count=N, offset=off).copy(); off += 8 * N
         modnum = np.frombuffer(raw, dtype="<u4", count=N, offset=off).copy(); off += 4 * N
-        bA = np.frombuffer(raw, dtype="<u4", count=int(nb), offset=off).copy(); off += 4 * int(nb)
-        iA = np.frombuffer(raw, dtype="<u4", count=N * speclen, offset=off).copy(); off += 4 * N * speclen
+        bA = iA = None
+        if full:
+            bA = np.frombuffer(raw, dtype="<u4", count=int(nb), offset=off).copy(); off += 4 * int(nb)
+            iA = np.frombuffer(raw, dtype="<u4", count=N * speclen, offset=off).copy(); off += 4 * N * speclen
         out.append(dict(L=L, N=N, npep=npep, speclen=speclen, seqs=seqs, mass=mass, seqid=seqid,
                         sites=sites, modnum=modnum, bA=bA, iA=iA))
     return dict(nlen=int(nlen), minlen=int(minlen), maxz=int(maxz), nbins=int(nb)), out

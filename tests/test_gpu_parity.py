@@ -11,11 +11,9 @@ import numpy as np
 import pytest
 
 import pyoracle
-from conftest import CASES, has_gpu, oracle_params, search_params
+from conftest import CASES, assert_same, has_gpu, oracle_params, search_params
 
 pytestmark = pytest.mark.gpu
-
-E_RTOL = 1e-9
 
 
 @pytest.fixture(scope="module")
@@ -24,38 +22,6 @@ def gx():
         pytest.skip("no CUDA device")
     import gicops_b200
     return gicops_b200
-
-
-def _heap_cells(arr):
-    return [(float(c["hyperscore"]), int(c["psid"]), int(c["idxoffset"]), int(c["sharedions"]), int(c["totalions"]))
-            for c in arr]
-
-
-def assert_same(res, heap, hist, ores, ohist, cap):
-    assert np.array_equal(res["cpsms"], ores["cpsms"])
-    assert np.array_equal(res["status"] & 7, ores["status"] & 7)
-    assert np.array_equal(hist, ohist)
-    for i in range(len(res)):
-        n = int(ores["heap_size"][i])
-        assert _heap_cells(heap[i][:n]) == _heap_cells(ores["heap"][i][:n]), i
-        assert np.all(heap[i][n:]["psid"] == 0)
-    m = (ores["status"] & 1) != 0
-    for f in ("psid", "idxoffset", "sharedions", "totalions"):
-        assert np.array_equal(res["top"][f][m], ores["top"][f][m]), f
-    assert np.array_equal(res["top"]["hyperscore"][m].view(np.uint32), ores["top"]["hyperscore"][m].view(np.uint32))
-    for f in ("maxhyp", "mu", "beta", "stt1", "end1"):
-        assert np.array_equal(res[f][m], ores[f][m]), f
-    ok = m & np.isfinite(ores["e_x"])
-    np.testing.assert_allclose(res["e_x"][ok], ores["e_x"][ok], rtol=E_RTOL)
-    np.testing.assert_allclose(res["slope"][ok], ores["slope"][ok], rtol=1e-12, atol=1e-15)
-    np.testing.assert_allclose(res["e_fp64"][ok], ores["e_fp64"][ok], rtol=E_RTOL)
-    if cap is not None:
-        rep = (res["status"] & 2) != 0
-        assert np.array_equal(rep, cap["cap_reported"] == 1)
-        assert np.array_equal(res["top"]["psid"][rep], cap["cap_psid"][rep])
-        assert np.array_equal(res["top"]["idxoffset"][rep], cap["cap_idxoffset"][rep])
-        assert np.array_equal(res["top"]["hyperscore"][rep].view(np.uint32), cap["cap_hyperscore"][rep].view(np.uint32))
-        np.testing.assert_allclose(res["e_x"][rep], cap["cap_e_x"][rep], rtol=E_RTOL)
 
 
 @pytest.mark.parametrize("case", CASES)
@@ -174,3 +140,45 @@ def test_gpu_min_cpsm_zero_and_one(gx, golden, flags):
         assert none.sum() > 0 and (~none).sum() > 0
         assert np.all((r.result["status"][none] & 1) == 0)
         assert np.all((r.result["status"][~none] & 1) != 0)
+
+
+@pytest.mark.parametrize("flags", [0, 2], ids=["batched", "plain"])
+def test_gpu_spectrum_over_peak_limit_gets_a_flagged_row(gx, golden, flags):
+    """A spectrum with more than GX_MAX_PEAKS peaks is not searched: through the device
+    entry point (which does not synchronise to read the guard word) its row is zero with
+    status GX_STATUS_PEAK_LIMIT, its histogram and heap rows are empty, and the spectra
+    around it are searched as usual."""
+    import torch
+    import gicops_b200._native as N
+    from conftest import concat_queries
+    c = golden("open_mox")
+    H, q0 = c["index"], c["queries"]
+    n = 1500
+    over = gx.synth.QueryBatch(np.array([0, n], np.uint32), np.arange(20000, 20000 + 5 * n, 5, dtype=np.int32),
+                               np.full(n, 3000, np.int32), np.array([1800.0], np.float32), np.array([3], np.int32),
+                               np.zeros(1, np.float32))
+    q = concat_queries(q0.subset(np.arange(10)), over, q0.subset(np.arange(10, 30)))
+    p = search_params(c, flags=flags)
+    dev = gx.DeviceIndex(H, 0)
+    s = gx.Searcher(dev, q.n, len(q.moz))
+    d = torch.device("cuda", 0)
+    t = {k: torch.from_numpy(np.ascontiguousarray(v)).to(d) for k, v in
+         dict(idx=q.idx.view(np.int32), moz=q.moz, intn=q.intn, prec=q.prec).items()}
+    out = torch.full((q.n * N.RESULT_DTYPE.itemsize,), 0x5A, dtype=torch.uint8, device=d)   # stale bytes
+    heap = torch.full((q.n * p.heap_cap * N.CELL_DTYPE.itemsize,), 0x5A, dtype=torch.uint8, device=d)
+    hist = torch.full((q.n * N.HIST_BINS,), 7, dtype=torch.int32, device=d)
+    s.search_device(dict(nspec=q.n, npeaks=len(q.moz), **{k: v.data_ptr() for k, v in t.items()}), p,
+                    out.data_ptr(), heap.data_ptr(), hist.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    r = out.cpu().numpy().view(N.RESULT_DTYPE)
+    assert r["status"][10] == N.STATUS_PEAK_LIMIT
+    z = r[10:11].copy()
+    z["status"] = 0
+    assert not np.any(z.view(np.uint8))
+    assert not np.any(hist.cpu().numpy().reshape(q.n, -1)[10])
+    assert not np.any(heap.cpu().numpy().reshape(q.n, -1)[10])
+    o, oh = pyoracle.search(H.lengths, q0.subset(np.arange(30)), oracle_params(c), hist=True)
+    keep = np.r_[0:10, 11:31]
+    assert np.array_equal(r["cpsms"][keep], o["cpsms"])
+    assert np.array_equal(hist.cpu().numpy().reshape(q.n, -1)[keep].view(np.uint32), oh)
+    assert np.count_nonzero(r["status"] & N.STATUS_PEAK_LIMIT) == 1

@@ -278,3 +278,30 @@ def test_workspace_attached_tail_matches_apply(torch, trained):
     ref = res_dev.cpu().numpy().view(N.RESULT_DTYPE)
     assert ((att["status"] & N.STATUS_LEARNED_TAIL) != 0).sum() > 10
     assert att.tobytes() == ref.tobytes()
+
+
+def test_tensor_core_wait_limit_gives_an_error_status(torch):
+    """A wait for the tensor core that runs out (limit 0: every wait gives up at once)
+    makes the GEMM record its guard, wait for the product it issued, free its tensor
+    memory and return.  gx_tail_check reports it once, and the next inference with the
+    normal limit gives the same output as before."""
+    import gicops_b200 as gx
+    import gicops_b200.tail as T
+    lib = gx.lib()
+    m = T.TailModel(0, max_batch=512, seed=5)
+    x = _bf16(torch, (300, 132), torch.Generator().manual_seed(3)).cuda()
+    good = m.predict(x).clone()
+    torch.cuda.synchronize()
+    assert lib.gx_tail_check(m.handle) == 0
+    try:
+        assert lib.gx_tail_set_wait_limit(0) == 0
+        m.predict(x)
+        rc = lib.gx_tail_check(m.handle)
+        msg = lib.gx_last_error()
+    finally:
+        lib.gx_tail_set_wait_limit(1_000_000_000)
+    assert rc == -3051 and b"tensor-core wait ran out" in msg
+    assert lib.gx_tail_check(m.handle) == 0          # reported once, then cleared
+    assert torch.equal(m.predict(x), good)
+    torch.cuda.synchronize()
+    m.close()

@@ -5,7 +5,10 @@ fixed-size array inside the library instead of a workspace.
 
 Checked here through the C ABI: two calls in a row give the same results as the
 allocating entry point (the array keeps the previous call's contents, so the second call
-shows that nothing stale leaks through), and batches beyond the array's size are refused.
+shows that nothing stale leaks through) -- on a golden case, on windows over several
+candidate tiles with per-spectrum tolerances (8- and 12-byte scorecards), and with a
+spectrum over the peak limit, which both entry points answer with a flagged empty row --
+and batches beyond the array's size are refused.
 This file is named so that pytest collects it last.
 """
 
@@ -19,29 +22,52 @@ from conftest import has_gpu, search_params
 pytestmark = pytest.mark.gpu
 
 
-def _dev_queries(q, torch, N):
+def _dev_queries(q, p, torch, N):
     d = torch.device("cuda", 0)
     t = dict(idx=torch.from_numpy(q.idx.view(np.int32).copy()).to(d), moz=torch.from_numpy(q.moz.copy()).to(d),
              intn=torch.from_numpy(q.intn.copy()).to(d), prec=torch.from_numpy(q.prec.copy()).to(d))
+    dm = None
+    if q.dM is not None:   # per-spectrum tolerances (Da); NaN takes the batch's
+        t["dM"] = torch.from_numpy(np.where(np.isnan(q.dM), p.dM, q.dM).astype(np.float64)).to(d)
+        dm = t["dM"].data_ptr()
     cq = N.Queries(q.n, len(q.moz), t["idx"].data_ptr(), t["moz"].data_ptr(), t["intn"].data_ptr(),
-                   t["prec"].data_ptr(), None, None)
+                   t["prec"].data_ptr(), None, dm)
     return cq, t
 
 
-def test_noalloc_matches_allocating_path(golden):
+def _case(name, golden, gx):
+    """(host index, queries, params) of a parity case."""
+    from conftest import MULTIBLOCK, concat_queries, multiblock_index, multiblock_queries
+    if name in ("open_mox", "peak_limit"):
+        c = golden("open_mox")
+        q = c["queries"]
+        if name == "peak_limit":   # one spectrum over GX_MAX_PEAKS: not searched, flagged
+            n = 1100
+            over = gx.synth.QueryBatch(np.array([0, n], np.uint32), np.arange(20000, 20000 + 7 * n, 7, dtype=np.int32),
+                                       np.full(n, 5000, np.int32), np.array([1500.0], np.float32),
+                                       np.array([2], np.int32), np.zeros(1, np.float32))
+            q = concat_queries(q.subset(np.arange(20)), over, q.subset(np.arange(20, 40)))
+        return c["index"], q, search_params(c, flags=gx.FLAG_PLAIN)
+    # windows over several 8,192-candidate tiles, half the spectra at +-10 ppm
+    H = multiblock_index(2)
+    q = multiblock_queries(H, 48, seed=51, window="mixed")
+    flags = gx.FLAG_PLAIN | (gx.FLAG_WIDE_SCORECARD if name == "multiblock_wide" else 0)
+    return H, q, gx.SearchParams(dM=MULTIBLOCK["dM"], expect_max=1e300, flags=flags)
+
+
+@pytest.mark.parametrize("name", ["open_mox", "multiblock", "multiblock_wide", "peak_limit"])
+def test_noalloc_matches_allocating_path(golden, name):
     if not has_gpu():
         pytest.skip("no CUDA device")
     import torch
     import gicops_b200 as gx
     import gicops_b200._native as N
 
-    c = golden("open_mox")
-    H, q = c["index"], c["queries"]
+    H, q, p = _case(name, golden, gx)
     dev = gx.DeviceIndex(H, 0)
     ws = gx.Searcher(dev, q.n, len(q.moz))
-    p = search_params(c, flags=gx.FLAG_PLAIN)
     cap = p.heap_cap
-    cq, keep = _dev_queries(q, torch, N)
+    cq, keep = _dev_queries(q, p, torch, N)
     cp = p.c()
     d = torch.device("cuda", 0)
 
@@ -64,6 +90,9 @@ def test_noalloc_matches_allocating_path(golden):
 
     rr = ref[0].cpu().numpy().view(N.RESULT_DTYPE)
     assert (rr["status"] & 1).sum() > 0
+    if name == "peak_limit":
+        assert rr["status"][20] == N.STATUS_PEAK_LIMIT and rr["cpsms"][20] == 0
+        assert np.count_nonzero(rr["status"] & N.STATUS_PEAK_LIMIT) == 1
     for o in runs:
         r = o[0].cpu().numpy().view(N.RESULT_DTYPE)
         for f in ("cpsms", "status", "maxhyp", "mu", "beta", "stt1", "end1"):
