@@ -232,16 +232,19 @@ def summarize_clocks(rows: list) -> dict:
             "reasons": reasons, "samples": len(rows)}
 
 
-def _harness_run(w: dict, db, sq, steps: int, warmup: int, cores: int, dM: float) -> list:
-    """Per-step query seconds of the reference harness on the batch sq at tolerance dM."""
+def _harness_run(w: dict, db, parts, steps: int, warmup: int, cores: int) -> list:
+    """Per-step query seconds of the reference harness: one index build, then per step every
+    (QueryBatch, tolerance in Da) part of `parts` searched in turn (their times summed)."""
     harness = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
     with tempfile.TemporaryDirectory() as tmp:
         dbdir = os.path.join(tmp, "db")
         db.write_peps(dbdir)
-        qf = os.path.join(tmp, "q.pbin")
-        sq.write_pbin(qf)
-        cmd = [harness, "--db", dbdir, "--maxz", str(w["maxz"]), "--dM", repr(float(dM)), "--dF", "5",
-               "--threads", str(cores), "--topmatches", "5", "--queries", qf, "--repeat", str(warmup + steps)]
+        cmd = [harness, "--db", dbdir, "--maxz", str(w["maxz"]), "--dF", "5", "--threads", str(cores),
+               "--topmatches", "5", "--repeat", str(warmup + steps)]
+        for i, (sq, dM) in enumerate(parts):
+            qf = os.path.join(tmp, f"q{i}.pbin")
+            sq.write_pbin(qf)
+            cmd += ["--batch", f"{qf}:{float(dM)!r}"]
         for r, m, n in w["mods"]:
             cmd += ["--mods", f"{r}:{m}:{n}"]
         if w["mods"]:
@@ -250,7 +253,8 @@ def _harness_run(w: dict, db, sq, steps: int, warmup: int, cores: int, dM: float
         if r.returncode != 0:
             raise RuntimeError(f"reference harness failed: {r.stderr[-400:]}")
         rec = json.loads(r.stdout.strip().splitlines()[-1])
-    log(f"[bench] reference CPU: {sq.n} spectra at dM {dM:g} Da x {len(rec['query_s_each'])} repeats, "
+    log(f"[bench] reference CPU: {sum(p[0].n for p in parts)} spectra in {len(parts)} batch(es) at dM "
+        f"{', '.join('%g' % p[1] for p in parts)} Da x {len(rec['query_s_each'])} repeats, "
         f"index build {rec['index_s']:.1f}s")
     return rec["query_s_each"][warmup:]
 
@@ -265,18 +269,16 @@ def reference_cpu(w: dict, db, q, sel, steps: int, warmup: int):
     sample = len(sel)
     sq = q.subset(sel)
     if sq.dM is None or np.all(np.isnan(sq.dM)):
-        each = _harness_run(w, db, sq, steps, warmup, cores, w["dM"])
+        parts = [(sq, w["dM"])]
     else:
         narrow = ~np.isnan(sq.dM)
-        parts = [(np.nonzero(~narrow)[0], w["dM"]), (np.nonzero(narrow)[0], float(np.median(sq.dM[narrow])))]
-        each = None
-        for idx, dm in parts:
-            if not len(idx):
-                continue
-            sub = sq.subset(idx)
-            sub.dM = None
-            e = np.asarray(_harness_run(w, db, sub, steps, warmup, cores, dm))
-            each = e if each is None else each + e
+        parts = []
+        for idx, dm in ((np.nonzero(~narrow)[0], w["dM"]), (np.nonzero(narrow)[0], float(np.median(sq.dM[narrow])))):
+            if len(idx):
+                sub = sq.subset(idx)
+                sub.dM = None
+                parts.append((sub, dm))
+    each = np.asarray(_harness_run(w, db, parts, steps, warmup, cores))
     per = float(np.mean(each))
     log(f"[bench] reference CPU: {sample} spectra, {per:.3f} s per step")
     return dict(value=sample / per, cores=cores, sample=sample, seconds=per, steps=len(each))

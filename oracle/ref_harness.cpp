@@ -18,8 +18,10 @@
 //               [--mods M:15.9949:2 ...] [--nmods 2] [--threads N] [--topmatches 5]
 //               [--expect-max 1e300] [--queries Q.pbin] [--first N] [--repeat R]
 //               [--out RES.bin] [--dump-index IDX.bin] [--qdm DM.f64]
-//               [--min-cpsm 4] [--min-shp 4] [--entries-only]
+//               [--min-cpsm 4] [--min-shp 4] [--entries-only] [--batch Q.pbin:DM ...]
 //   ref_harness --ms2-to-pbin FILE.ms2     (the reference's MS2 conversion: FILE.ms2.pbin)
+// --batch (repeatable) searches several query files, each at its own global tolerance DM
+// (Da), against one index build; each repeat runs them all and is timed as their sum.
 // --entries-only stops after the index entries (LBE_* steps, no fragment-ion index) and,
 // with --dump-index, writes them alone (magic GXREFEN1: no bA / iA arrays).
 // --qdm gives one precursor tolerance (Da, float64) per spectrum: each spectrum is then
@@ -138,6 +140,7 @@ int main(int argc, char **argv)
 {
     std::string db, qpath, outpath, dumppath, qdmpath, ms2path;
     std::vector<std::string> mods;
+    std::vector<std::pair<std::string, double>> batches;   // --batch PATH:DM
     int minlen = 6, maxlen = 46, maxz = 1, nmods = 0, threads = omp_get_max_threads();
     int topmatches = 5, first = -1, repeat = 1, min_cpsm = 4, min_shp = 4;
     double dM = 10.0, expect_max = 1e300;
@@ -171,6 +174,12 @@ int main(int argc, char **argv)
         else if (a == "--min-shp") min_shp = std::atoi(nxt().c_str());
         else if (a == "--ms2-to-pbin") ms2path = nxt();
         else if (a == "--entries-only") entries_only = true;
+        else if (a == "--batch") {
+            const std::string v = nxt();
+            const size_t c = v.rfind(':');
+            if (c == std::string::npos) { std::fprintf(stderr, "--batch wants PATH:DM\n"); return 2; }
+            batches.emplace_back(v.substr(0, c), std::atof(v.c_str() + c + 1));
+        }
         else { std::fprintf(stderr, "unknown option %s\n", a.c_str()); return 2; }
     }
     if (!ms2path.empty()) {
@@ -282,11 +291,17 @@ int main(int argc, char **argv)
     double tq = 0.0;
     std::vector<double> t_each;
     size_t nspec = 0;
-    if (!qpath.empty() && !entries_only) {
-        std::vector<Spec> specs;
-        if (!read_pbin(qpath, specs)) { std::fprintf(stderr, "bad pbin %s\n", qpath.c_str()); return 1; }
-        if (first >= 0 && (size_t)first < specs.size()) specs.resize(first);
-        nspec = specs.size();
+    if (!qpath.empty()) batches.insert(batches.begin(), std::make_pair(qpath, dM));
+    if (!batches.empty() && !entries_only) {
+        // every batch read up front; with a single batch, --first and --qdm apply to it
+        std::vector<std::vector<Spec>> all(batches.size());
+        for (size_t bi = 0; bi < batches.size(); bi++)
+            if (!read_pbin(batches[bi].first, all[bi])) {
+                std::fprintf(stderr, "bad pbin %s\n", batches[bi].first.c_str());
+                return 1;
+            }
+        if (first >= 0 && all.size() == 1 && (size_t)first < all[0].size()) all[0].resize(first);
+        for (auto &v : all) nspec += v.size();
         g_capture.assign(nspec, Capture{});
 
         SchedHandle = new Scheduler(0);
@@ -295,7 +310,8 @@ int main(int argc, char **argv)
         Queries<int> q;
         const int chunk = QCHUNK;
         size_t maxpk = 0;
-        for (auto &s : specs) maxpk = std::max(maxpk, s.mz.size());
+        for (auto &v : all)
+            for (auto &sp : v) maxpk = std::max(maxpk, sp.mz.size());
         q.idx = new uint_t[chunk + 1];
         q.precurse = new float_t[chunk];
         q.charges = new int_t[chunk];
@@ -305,6 +321,7 @@ int main(int argc, char **argv)
 
         std::vector<double> qdm;
         if (!qdmpath.empty()) {
+            if (all.size() != 1) { std::fprintf(stderr, "--qdm needs a single batch\n"); return 1; }
             qdm.resize(nspec);
             FILE *f = std::fopen(qdmpath.c_str(), "rb");
             if (!f || std::fread(qdm.data(), 8, nspec, f) != nspec) { std::fprintf(stderr, "bad --qdm\n"); return 1; }
@@ -313,29 +330,35 @@ int main(int argc, char **argv)
         const size_t step = qdm.empty() ? (size_t)chunk : 1;
         for (int r = 0; r < repeat; r++) {
             const double tq0 = tq;
-            for (size_t b0 = 0; b0 < nspec; b0 += step) {
-                const size_t b1 = std::min(nspec, b0 + step);
-                if (!qdm.empty()) params.dM = qdm[b0];
-                size_t ind = 0;
-                q.idx[0] = 0;
-                for (size_t s = b0; s < b1; s++) {
-                    const Spec &sp = specs[s];
-                    q.precurse[s - b0] = sp.prec;
-                    q.charges[s - b0] = sp.z;
-                    q.rtimes[s - b0] = sp.rt;
-                    std::memcpy(q.moz + ind, sp.mz.data(), 4 * sp.mz.size());
-                    std::memcpy(q.intensity + ind, sp.in.data(), 4 * sp.in.size());
-                    ind += sp.mz.size();
-                    q.idx[s - b0 + 1] = (uint_t)ind;
+            size_t base = 0;   // spectrum id of the batch's first spectrum (capture order)
+            for (size_t bi = 0; bi < all.size(); bi++) {
+                const std::vector<Spec> &specs = all[bi];
+                params.dM = batches[bi].second;
+                for (size_t b0 = 0; b0 < specs.size(); b0 += step) {
+                    const size_t b1 = std::min(specs.size(), b0 + step);
+                    if (!qdm.empty()) params.dM = qdm[b0];
+                    size_t ind = 0;
+                    q.idx[0] = 0;
+                    for (size_t s = b0; s < b1; s++) {
+                        const Spec &sp = specs[s];
+                        q.precurse[s - b0] = sp.prec;
+                        q.charges[s - b0] = sp.z;
+                        q.rtimes[s - b0] = sp.rt;
+                        std::memcpy(q.moz + ind, sp.mz.data(), 4 * sp.mz.size());
+                        std::memcpy(q.intensity + ind, sp.in.data(), 4 * sp.in.size());
+                        ind += sp.mz.size();
+                        q.idx[s - b0 + 1] = (uint_t)ind;
+                    }
+                    q.numPeaks = (int)ind;
+                    q.numSpecs = (int)(b1 - b0);
+                    q.batchNum = (int)(b0 / chunk);
+                    q.fileNum = 0;
+                    double a = now_s();
+                    st = DSLIM_QuerySpectrum(&q, index, (uint_t)nlen, (int)(base + b0));
+                    tq += now_s() - a;
+                    if (st != SLM_SUCCESS) { std::fprintf(stderr, "query failed: %d\n", st); return 1; }
                 }
-                q.numPeaks = (int)ind;
-                q.numSpecs = (int)(b1 - b0);
-                q.batchNum = (int)(b0 / chunk);
-                q.fileNum = 0;
-                double a = now_s();
-                st = DSLIM_QuerySpectrum(&q, index, (uint_t)nlen, (int)b0);
-                tq += now_s() - a;
-                if (st != SLM_SUCCESS) { std::fprintf(stderr, "query failed: %d\n", st); return 1; }
+                base += specs.size();
             }
             t_each.push_back(tq - tq0);
         }
