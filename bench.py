@@ -379,8 +379,10 @@ def main():
     ap.add_argument("--spectra", type=int, default=0, help="search only the first N spectra (profiling cases)")
     ap.add_argument("--no-tail", action="store_true", help="leave the learned tail out of the step")
     ap.add_argument("--no-index-build", action="store_true", help="skip timing the GPU index build at set-up")
-    ap.add_argument("--sparse-below", type=int, default=500,
-                    help="queries with fewer candidate PSMs take the learned tail")
+    ap.add_argument("--sparse-below", type=int, default=0,
+                    help="queries with fewer candidate PSMs take the learned tail (0: calibrated)")
+    ap.add_argument("--tail-queries", type=int, default=16000,
+                    help="well-populated queries the learned tail is trained on (64 subsamples each)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -469,7 +471,10 @@ def main():
     t_out = torch.empty(q.n * N.RESULT_DTYPE.itemsize, dtype=torch.uint8, device=d)
     t_hist = torch.empty((q.n, N.HIST_BINS), dtype=torch.int32, device=d)
 
-    # ---- learned tail: trained here (untimed) on this workload's well-populated queries --
+    # ---- learned tail: trained here (untimed) on this workload's well-populated queries:
+    # subsamples of their histograms against the plain fit of all their candidates; the
+    # candidate threshold below which the model replaces the plain fit is calibrated on
+    # other such queries, and the gain reported on a third, held-out set ------------------
     tail = None
     tail_info = None
     if not args.no_tail and not args.plain:
@@ -480,21 +485,37 @@ def main():
         res0 = t_out.cpu().numpy().view(N.RESULT_DTYPE)
         pop = np.nonzero(((res0["status"] & 1) != 0) & (res0["cpsms"] >= 10000) & np.isfinite(res0["slope"]) &
                          (res0["slope"] < 0))[0]
-        rng = np.random.default_rng(7)
-        pop = rng.permutation(pop)[:4000]
-        tail = T.TailModel(local, max_batch=8192, seed=11)
-        if len(pop) >= 64:
+        pop = np.random.default_rng(7).permutation(pop)
+        held, calib, train = pop[:300], pop[300:600], pop[600:600 + args.tail_queries]
+        if len(train) >= 64:
+            tail = T.TailModel(local, max_batch=8192, seed=11)
+            tail.set_loss(0.5)
             dv = dict(hist=t_hist, res=t_out, prec=t_pre, charge=t_chg)
-            smp = T.plan(pop, per_query=32, keep_range=(8, 512), seed=1)
+            smp = T.plan(train, per_query=64, keep_range=(8, 512), seed=1)
             xs, ts = T.training_set(tail, dv, res0, smp)
             tail.set_norm_from(ts.cpu().numpy())
-            losses = tail.train(xs, ts, epochs=6, batch=512, opt=T.Adam(lr=1e-3), seed=2, lr_decay=0.8)
-            tail_info = {"sparse_below": args.sparse_below, "train_queries": int(len(pop)),
-                         "train_samples": int(len(smp)), "train_loss": [round(x, 4) for x in losses],
-                         "train_s": round(time.perf_counter() - t0, 2)}
-            ws.set_tail(tail, args.sparse_below)   # every search below applies it after the plain fit
-        else:
-            tail = None
+            losses = tail.train(xs, ts, epochs=6, batch=512, opt=T.Adam(lr=1e-3, w_slope=0.2), seed=2, lr_decay=0.8)
+            del xs, ts
+            cal = T.evaluate(tail, dv, res0, T.plan(calib, per_query=8, keep_range=(20, 500), seed=4))
+            below = args.sparse_below or T.choose_sparse_below(cal["err_plain"], cal["err_learned"], cal["cpsms_sub"])
+            ev = T.evaluate(tail, dv, res0, T.plan(held, per_query=8, keep_range=(20, 500), seed=3))
+            m = ev["cpsms_sub"] < below
+            qf = lambda e, f: round(float(np.quantile(e, f)), 3) if len(e) else None  # noqa: E731
+            ep, el = ev["err_plain"][m], ev["err_learned"][m]
+            tail_info = {"sparse_below": int(below), "sparse_below_from": "argument" if args.sparse_below else
+                         "calibration (300 held-out well-populated queries subsampled to 20-500 candidates)",
+                         "loss": "huber 0.5", "train_queries": int(len(train)), "train_samples": int(len(smp)),
+                         "train_loss": [round(x, 4) for x in losses], "train_s": round(time.perf_counter() - t0, 2),
+                         "held_out": {"queries": int(len(held)), "subsamples_below_threshold": int(m.sum()),
+                                      "abs_log10_e_error_vs_full_fit": {
+                                          "plain": {"median": qf(ep, .5), "p90": qf(ep, .9), "p99": qf(ep, .99)},
+                                          "learned": {"median": qf(el, .5), "p90": qf(el, .9), "p99": qf(el, .99)}},
+                                      "share_within_0.1_log10": {"plain": float(np.mean(ep <= .1)) if len(ep) else None,
+                                                                 "learned": float(np.mean(el <= .1)) if len(el) else None}}}
+            if below > 0:
+                ws.set_tail(tail, below)   # every search below applies it after the plain fit
+            else:
+                tail = None
         log(f"[bench] learned tail: {tail_info}")
 
     def step():

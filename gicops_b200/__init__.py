@@ -10,7 +10,7 @@ from . import prep, synth, tail
 from ._native import (CELL_DTYPE, FLAG_PLAIN, FLAG_WIDE_SCORECARD, HIST_BINS, PEP_ENTRY_DTYPE, RESULT_DTYPE,
                       GxError, lib)
 from .index import DeviceIndex, HostIndex
-from .search import Searcher, SearchParams, SearchResults
+from .search import Searcher, SearchParams, SearchResults, Streamer
 
 __all__ = ["synth", "tail", "lib", "GxError", "HostIndex", "DeviceIndex", "Searcher", "SearchParams", "SearchResults",
-           "RESULT_DTYPE", "CELL_DTYPE", "PEP_ENTRY_DTYPE", "HIST_BINS", "FLAG_PLAIN", "FLAG_WIDE_SCORECARD"]
+           "Streamer", "RESULT_DTYPE", "CELL_DTYPE", "PEP_ENTRY_DTYPE", "HIST_BINS", "FLAG_PLAIN", "FLAG_WIDE_SCORECARD"]

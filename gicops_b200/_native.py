@@ -100,6 +100,11 @@ class Queries(C.Structure):
                 ("intn", C.c_void_p), ("prec", C.c_void_p), ("charge", C.c_void_p), ("dM", C.c_void_p)]
 
 
+class StreamStats(C.Structure):
+    _fields_ = [("chunks", C.c_uint32), ("pad", C.c_uint32), ("total_ms", C.c_double), ("upload_ms", C.c_double),
+                ("search_ms", C.c_double), ("download_ms", C.c_double)]
+
+
 class TailAdam(C.Structure):
     _fields_ = [("lr", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float),
                 ("w_slope", C.c_float), ("w_lgs", C.c_float)]
@@ -139,6 +144,11 @@ _SIGS = [
                                      C.c_void_p, C.c_void_p, C.c_void_p]),
     ("gx_search_device_noalloc", C.c_int32, [C.c_void_p, C.POINTER(Queries), C.POINTER(Params), C.c_void_p,
                                              C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("gx_streamer_create", C.c_int32, [C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(C.c_void_p)]),
+    ("gx_streamer_free", C.c_int32, [C.c_void_p]),
+    ("gx_streamer_workspace", C.c_void_p, [C.c_void_p]),
+    ("gx_search_stream", C.c_int32, [C.c_void_p, C.POINTER(Queries), C.POINTER(Params), C.c_void_p,
+                                     C.POINTER(StreamStats)]),
     ("gx_traffic_host", C.c_int32, [C.POINTER(LengthDesc), C.c_int32, C.POINTER(Queries), C.POINTER(Params),
                                     C.c_void_p, C.c_void_p, C.c_int32]),
     ("gx_heap_capacity", C.c_int32, [C.c_uint32]),
@@ -162,6 +172,7 @@ _SIGS = [
                                   C.c_uint32, C.c_double, C.c_void_p]),
     ("gx_tail_check", C.c_int32, [C.c_void_p]),
     ("gx_tail_set_wait_limit", C.c_int32, [C.c_uint64]),
+    ("gx_tail_set_loss", C.c_int32, [C.c_void_p, C.c_float]),
     ("gx_workspace_set_tail", C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32]),
     ("gx_tail_gemm", C.c_int32, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_int64, C.c_int64, C.c_int32,
                                  C.c_int32, C.c_int32, C.c_void_p, C.c_int64, C.c_void_p]),

@@ -22,4 +22,13 @@ void count_launch(uint64_t n = 1);
 int prof_begin(const char *name, void *stream);
 void prof_end(int handle, void *stream);
 
+// Search of a batch already in device memory through a workspace, on `stream` (the
+// launch sequence of gx_search_device after its argument checks; the index's device must
+// be current).  heap / hist may be NULL.
+gx_status search_launch(gx_index *ix, gx_workspace *ws, const gx_queries *q_dev, const gx_params *p, gx_result *out,
+                        gx_cell *heap, uint32_t *hist, void *stream);
+// The workspace's own stream, and its device guard word (device memory, int32).
+void *workspace_stream(gx_workspace *ws);
+int32_t *workspace_err(gx_workspace *ws);
+
 }  // namespace gx

@@ -614,6 +614,16 @@ gx_status launch_search(gx_index *ix, gx_workspace *ws, const gx_queries *q, con
 
 }  // namespace
 
+namespace gx {
+gx_status search_launch(gx_index *ix, gx_workspace *ws, const gx_queries *q_dev, const gx_params *p, gx_result *out,
+                        gx_cell *heap, uint32_t *hist, void *stream)
+{
+    return launch_search(ix, ws, q_dev, p, out, heap, hist, (cudaStream_t)stream);
+}
+void *workspace_stream(gx_workspace *ws) { return ws->stream; }
+int32_t *workspace_err(gx_workspace *ws) { return ws->err; }
+}  // namespace gx
+
 extern "C" gx_status gx_workspace_set_tail(gx_workspace *ws, gx_tail_model *m, uint32_t sparse_below)
 {
     if (!ws) return fail(GX_ERR_INVLD_PTR, "gx_workspace_set_tail: null workspace");
@@ -649,6 +659,8 @@ extern "C" gx_status gx_search_host(gx_index *ix, gx_workspace *ws, const gx_que
     GX_CUDA(ds.status());
     cudaStream_t st = ws->stream;
     const uint32_t n = q->nspec;
+    // the guard word may hold a flag of an earlier gx_search_device call, which reports none
+    GX_CUDA(cudaMemsetAsync(ws->err, 0, sizeof(int32_t), st));
     if (heap_out && !ws->heap) GX_CUDA(cudaMalloc(&ws->heap, sizeof(gx_cell) * GX_MAX_HEAP * (uint64_t)ws->max_spec));
     if (hist_out && !ws->hist) GX_CUDA(cudaMalloc(&ws->hist, sizeof(uint32_t) * GX_HIST_BINS * (uint64_t)ws->max_spec));
     GX_CUDA(cudaMemcpyAsync(ws->qidx, q->idx, sizeof(uint32_t) * (n + 1), cudaMemcpyHostToDevice, st));

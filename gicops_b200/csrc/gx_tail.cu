@@ -16,7 +16,7 @@
 //                candidates to `keep` (exact sampling without replacement, Floyd's method)
 //   k_fit_rows   plain FP64 expeRT fit of arbitrary histogram rows
 //   k_gemm       tcgen05 GEMM + epilogue (bias, GELU, GELU', fp32 / bf16 stores)
-//   k_loss       weighted squared error on normalised targets, its gradient in bf16
+//   k_loss       weighted squared error or Huber loss on normalised targets, its gradient in bf16
 //   k_colsum     bias gradients (column sums, fixed order)
 //   k_adam       Adam step on the fp32 master weights + bf16 copies
 //   k_predict    de-normalised predictions (slope, log10 survival at the top bin)
@@ -389,10 +389,11 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(GemmArgs a)
 // ------------------------------------------------------------------------------------
 // small kernels
 // ------------------------------------------------------------------------------------
-// loss = sum_i sum_o w_o (y_io - t'_io)^2 / n with t' = (t - mean_o) / std_o;
-// dY = 2 w_o (y - t') / n in bf16
-__global__ void k_loss(const float *Y, const float *T, uint32_t n, const float *norm, float w0, float w1, bf16 *dY,
-                       float *loss)
+// loss = sum_i sum_o w_o rho(y_io - t'_io) / n with t' = (t - mean_o) / std_o and dY its
+// gradient in bf16.  rho(d) = d^2 (huber = 0), or Huber's loss with that delta:
+// d^2 / (2 huber) for |d| < huber, |d| - huber / 2 beyond (gradient d / huber, then +-1).
+__global__ void k_loss(const float *Y, const float *T, uint32_t n, const float *norm, float w0, float w1,
+                       float huber, bf16 *dY, float *loss)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     float l = 0.0f;
@@ -402,8 +403,21 @@ __global__ void k_loss(const float *Y, const float *T, uint32_t n, const float *
         for (int o = 0; o < 2; o++) {
             const float t = (T[2 * (size_t)i + o] - norm[2 * o]) / norm[2 * o + 1];
             const float d = Y[2 * (size_t)i + o] - t;
-            l += w[o] * d * d;
-            dY[2 * (size_t)i + o] = __float2bfloat16_rn(2.0f * w[o] * d / (float)n);
+            float g;
+            if (huber > 0.0f) {
+                const float ad = fabsf(d);
+                if (ad < huber) {
+                    l += w[o] * (0.5f * d * d / huber);
+                    g = w[o] * d / huber;
+                } else {
+                    l += w[o] * (ad - 0.5f * huber);
+                    g = d > 0.0f ? w[o] : -w[o];
+                }
+            } else {
+                l += w[o] * d * d;
+                g = 2.0f * w[o] * d;
+            }
+            dY[2 * (size_t)i + o] = __float2bfloat16_rn(g / (float)n);
         }
     }
 #pragma unroll
@@ -494,6 +508,7 @@ struct gx_tail_model {
     uint32_t max_batch = 0;
     uint64_t step = 0;
     float norm_h[4] = {0.f, 1.f, 0.f, 1.f};
+    float huber = 0.0f;   // training loss: 0 squared error, > 0 Huber's loss with this delta
     float *P = nullptr, *G = nullptr, *m1 = nullptr, *m2 = nullptr, *norm = nullptr;
     bf16 *Pb = nullptr;
     float *Z1 = nullptr, *Z2 = nullptr, *Y = nullptr, *loss = nullptr, *pred = nullptr;
@@ -591,7 +606,7 @@ gx_status grads(gx_tail_model *m, const bf16 *X, const float *T, uint32_t n, flo
 {
     GX_TRY(forward(m, X, n, st));
     int h = prof_begin("k_loss", st);
-    k_loss<<<blocks(n, 256), 256, 0, st>>>(m->Y, T, n, m->norm, w0, w1, m->dY, m->loss);
+    k_loss<<<blocks(n, 256), 256, 0, st>>>(m->Y, T, n, m->norm, w0, w1, m->huber, m->dY, m->loss);
     prof_end(h, st);
     GX_TRY(launched("tail model: k_loss"));
     float *G = m->G;
@@ -868,6 +883,15 @@ extern "C" gx_status gx_tail_check(gx_tail_model *m)
     if ((e = cudaMemset(m->err, 0, sizeof(int32_t))) != cudaSuccess) return cuda_fail(e, "gx_tail_check: clear");
     if (v == 1) return fail(GX_ERR_DEVICE_GUARD, "tail model: a sample had an invalid top bin");
     return fail(GX_ERR_DEVICE_GUARD, "tail model: a tensor-core wait ran out");
+}
+
+extern "C" gx_status gx_tail_set_loss(gx_tail_model *m, float huber_delta)
+{
+    if (!m) return fail(GX_ERR_INVLD_PTR, "gx_tail_set_loss: null model");
+    if (!(huber_delta >= 0.0f) || !std::isfinite(huber_delta))
+        return fail(GX_ERR_INVLD_PARAM, "gx_tail_set_loss: the Huber delta must be finite and >= 0");
+    m->huber = huber_delta;
+    return GX_SUCCESS;
 }
 
 extern "C" gx_status gx_tail_set_wait_limit(uint64_t ns)

@@ -108,6 +108,49 @@ class Searcher:
                                          hist_dev, stream))
 
 
+class Streamer:
+    """Chunked search of a host batch (gx_streamer): chunk i+1's upload and chunk i-1's
+    result download overlap chunk i's search.  Results equal one search of the whole
+    batch.  The batch's arrays should be pinned for the copies to overlap."""
+
+    def __init__(self, index: DeviceIndex, chunk: int = 65536, max_peaks: int = 0):
+        self.index = index
+        self.chunk = chunk
+        self.handle = C.c_void_p()
+        N.check(N.lib().gx_streamer_create(index.handle, chunk, max_peaks, C.byref(self.handle)))
+
+    def close(self) -> None:
+        if self.handle:
+            N.lib().gx_streamer_free(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_tail(self, model, sparse_below: int = 500) -> None:
+        """As Searcher.set_tail, for every chunk's search."""
+        ws = N.lib().gx_streamer_workspace(self.handle)
+        N.check(N.lib().gx_workspace_set_tail(ws, model.handle if model else None, sparse_below))
+        self._tail = model
+
+    def search(self, q: QueryBatch, params: SearchParams, out=None, stats: bool = False):
+        """Results (gx_result records, host) of the batch; with stats also the timing
+        dict (chunks, total/upload/search/download ms).  `out` may be a preallocated
+        (pinned) record array."""
+        cq, keep = make_c_queries(q, params)
+        res = np.zeros(q.n, N.RESULT_DTYPE) if out is None else out
+        p = params.c()
+        st = N.StreamStats()
+        N.check(N.lib().gx_search_stream(self.handle, C.byref(cq), C.byref(p), res.ctypes.data,
+                                         C.byref(st) if stats else None))
+        if not stats:
+            return res
+        return res, {f: getattr(st, f) for f in ("chunks", "total_ms", "upload_ms", "search_ms", "download_ms")}
+
+
 def make_c_queries(q: QueryBatch, params: SearchParams):
     """C view of a QueryBatch (host arrays); returns (struct, keep-alive list)."""
     idx = np.ascontiguousarray(q.idx, np.uint32)

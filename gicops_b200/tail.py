@@ -116,6 +116,11 @@ class TailModel:
         d = np.load(path)
         self.set(d["params"], d["norm"])
 
+    def set_loss(self, huber: float = 0.0) -> None:
+        """Training loss: the squared error (0) or Huber's loss with this delta, in
+        normalised target units (gx_tail_set_loss)."""
+        check(lib().gx_tail_set_loss(self.handle, float(huber)))
+
     def set_norm_from(self, targets) -> np.ndarray:
         """Target normalisation (mean, scale per output) from a training set's targets."""
         t = np.asarray(targets, dtype=np.float64)
@@ -235,6 +240,24 @@ def training_set(model: TailModel, dev: dict, res_host: np.ndarray, smp: np.ndar
     r = res_host[smp["query"]]
     t = torch.from_numpy(line_targets(r["slope"], r["icpt"], r["maxhyp"])).to(x.device)
     return x, t
+
+
+def choose_sparse_below(err_plain, err_learned, cands, thresholds=(25, 50, 75, 100, 150, 200, 300, 500),
+                        min_rows: int = 100) -> int:
+    """The fallback policy's candidate threshold, from calibration samples (held-out
+    well-populated queries subsampled to sparsity, errors against their full-data fit): the
+    largest threshold T for which the samples with fewer than T candidates have a smaller
+    median AND a smaller 90th-percentile error with the learned line than with the plain
+    fit.  0 when no threshold qualifies: the model is then never used."""
+    ep, el, cs = (np.asarray(a) for a in (err_plain, err_learned, cands))
+    best = 0
+    for t in sorted(thresholds):
+        m = cs < t
+        if m.sum() < min_rows:
+            continue
+        if np.median(el[m]) < np.median(ep[m]) and np.quantile(el[m], 0.9) < np.quantile(ep[m], 0.9):
+            best = t
+    return int(best)
 
 
 def evaluate(model: TailModel, dev: dict, res_host: np.ndarray, smp: np.ndarray) -> dict:

@@ -276,6 +276,39 @@ gx_status gx_search_device(gx_index *ix, gx_workspace *ws, const gx_queries *q_d
 gx_status gx_search_device_noalloc(gx_index *ix, const gx_queries *q_dev, const gx_params *p, gx_result *out_dev,
                                    gx_cell *heap_dev, uint32_t *hist_dev, void *stream);
 
+/* ---- streamed search of a batch in host memory --------------------------------------
+ * Replaces the reference's batch feed to its GPU path: a ring of host query buffers
+ * (source/core/dslim_query.cpp:183-203), each batch uploaded synchronously before its
+ * search (dQueries::H2D, source/core/cuda/superstep3/kernel.cu:192-206).  A streamer owns
+ * a workspace for `chunk` spectra and two sets of device query and result buffers: a host
+ * batch of any size is searched chunk by chunk, the upload of one chunk (one
+ * cudaMemcpyAsync per array, on an upload stream) and the download of another's results
+ * (a download stream) overlapping the search of a third (the workspace's stream).  The
+ * results equal one gx_search_device call over the whole batch.  Host arrays should be
+ * pinned (cudaHostAlloc / cudaHostRegister) for the copies to overlap; pageable memory
+ * gives the same results with the copies serialised.  max_peaks = peaks per chunk the
+ * buffers hold (0: chunk * 160).  A learned tail is attached through
+ * gx_workspace_set_tail(gx_streamer_workspace(s), ...). */
+typedef struct gx_streamer gx_streamer;
+typedef struct {
+    uint32_t chunks;
+    uint32_t pad;
+    double total_ms;      /* first upload to last download, GPU clock */
+    double upload_ms;     /* summed over chunks: host-to-device copies */
+    double search_ms;     /* summed over chunks: the search launch sequence */
+    double download_ms;   /* summed over chunks: device-to-host copies of the results */
+} gx_stream_stats;
+gx_status gx_streamer_create(gx_index *ix, uint32_t chunk, uint32_t max_peaks, gx_streamer **out);
+gx_status gx_streamer_free(gx_streamer *s);
+gx_workspace *gx_streamer_workspace(gx_streamer *s);
+/* Search q (HOST arrays, idx[0] = 0) into out (HOST, q->nspec records); stats may be NULL
+ * (when given, each chunk's copies and search are timed with events, which adds a little
+ * host overhead).  Synchronises before returning; GX_ERR_DEVICE_GUARD if a spectrum had
+ * more than GX_MAX_PEAKS peaks (its record carries GX_STATUS_PEAK_LIMIT), GX_ERR_INVLD_SIZE
+ * before any work if a chunk holds more peaks than the streamer's buffers. */
+gx_status gx_search_stream(gx_streamer *s, const gx_queries *q, const gx_params *p, gx_result *out,
+                           gx_stream_stats *stats);
+
 /* Algorithmic traffic of the path, per spectrum (host arrays, for roofline figures):
  * ids_out[s] = ion ids inside the precursor window of every distinct probed bin,
  * bins_out[s] = distinct probed bins, both summed over lengths with a non-empty
@@ -366,6 +399,12 @@ gx_status gx_tail_fit_rows(const uint32_t *hist_dev, const int32_t *cpsms_dev, c
  * mean loss.  weights2 (host, optional) = loss weights of the two outputs (default 1, 1). */
 gx_status gx_tail_grad(gx_tail_model *m, const uint16_t *x_dev, const float *target_dev, uint32_t n,
                        const float *weights2, float *grad_dev, float *loss_dev, void *stream);
+/* Training loss of gx_tail_grad / gx_tail_train_step, per normalised output d = y - t:
+ * huber_delta = 0 (the default) the squared error d^2; > 0 Huber's loss, d^2 / (2 delta) for
+ * |d| < delta and |d| - delta / 2 beyond.  Huber's loss follows the median of a heavy-tailed
+ * target (the full-data fit of a sparse query's histogram varies by orders of magnitude)
+ * where the squared error follows its mean. */
+gx_status gx_tail_set_loss(gx_tail_model *m, float huber_delta);
 /* One Adam step on a batch (gx_tail_grad followed by the update). */
 gx_status gx_tail_train_step(gx_tail_model *m, const uint16_t *x_dev, const float *target_dev, uint32_t n,
                              const gx_tail_adam *opt, float *loss_dev, void *stream);

@@ -131,8 +131,10 @@ def forward(P, X, emulate: bool = True) -> dict:
     return dict(Xb=Xb, W1=W1, W2=W2, W3=W3, Z1=Z1, A1=A1, Z2=Z2, A2=A2, Y=Y)
 
 
-def loss_and_grads(P, X, T, norm, w=(1.0, 1.0), emulate: bool = True) -> tuple[float, np.ndarray]:
-    """Mean weighted squared error on normalised targets and its gradient (flat, NPARAM)."""
+def loss_and_grads(P, X, T, norm, w=(1.0, 1.0), emulate: bool = True, huber: float = 0.0) -> tuple[float, np.ndarray]:
+    """Mean weighted loss on normalised targets and its gradient (flat, NPARAM): the squared
+    error (huber 0) or Huber's loss with delta huber (d^2 / 2 delta inside, |d| - delta / 2
+    outside), as k_loss computes them."""
     r = bf16 if emulate else (lambda v: np.asarray(v, dtype=np.float64))
     f = forward(P, X, emulate)
     n = X.shape[0]
@@ -140,8 +142,14 @@ def loss_and_grads(P, X, T, norm, w=(1.0, 1.0), emulate: bool = True) -> tuple[f
     tn = np.stack([(T[:, 0] - norm[0]) / norm[1], (T[:, 1] - norm[2]) / norm[3]], axis=1)
     wv = np.asarray(w, dtype=np.float64)
     d = f["Y"] - tn
-    loss = float((wv * d * d).sum() / n)
-    dY = r(2.0 * wv * d / n)
+    if huber > 0:
+        ad = np.abs(d)
+        inside = ad < huber
+        loss = float((wv * np.where(inside, 0.5 * d * d / huber, ad - 0.5 * huber)).sum() / n)
+        dY = r(wv * np.where(inside, d / huber, np.sign(d)) / n)
+    else:
+        loss = float((wv * d * d).sum() / n)
+        dY = r(2.0 * wv * d / n)
     g = {}
     g["W3"] = dY.T @ f["A2"]
     g["b3"] = dY.sum(axis=0)

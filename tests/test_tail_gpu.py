@@ -109,10 +109,12 @@ def test_features_and_fits_match_oracle(torch, searched):
     assert np.array_equal(fit[full, 1], res[smp["query"][full]]["icpt"])
 
 
-def test_gradients_match_oracle(torch, searched):
+@pytest.mark.parametrize("huber", [0.0, 0.5], ids=["squared", "huber"])
+def test_gradients_match_oracle(torch, searched, huber):
     import gicops_b200.tail as T
     import tail_mlp as O
     m = T.TailModel(0, max_batch=512, seed=3)
+    m.set_loss(huber)
     smp = _sample_table(searched["res"], seed=6)[:448]
     dv = searched["dev"]
     x = m.features(dv["hist"], dv["res"], dv["prec"], dv["charge"], smp)
@@ -125,7 +127,8 @@ def test_gradients_match_oracle(torch, searched):
     torch.cuda.synchronize()
     P, _, _ = m.get()
     xv = O.bf16_value(x.view(torch.int16).cpu().numpy().view(np.uint16))
-    l_o, g_o = O.loss_and_grads(P.astype(np.float64), xv, tgt, norm.astype(np.float64), w, emulate=True)
+    l_o, g_o = O.loss_and_grads(P.astype(np.float64), xv, tgt, norm.astype(np.float64), w, emulate=True,
+                                huber=huber)
     g = g.cpu().numpy().astype(np.float64)
     assert abs(float(loss.item()) - l_o) <= 1e-4 * abs(l_o)
     o = 0
@@ -136,7 +139,8 @@ def test_gradients_match_oracle(torch, searched):
         assert err < 2e-3, (name, err)
         o += n
     # the bf16 network against the unrounded FP64 one: the rounding's own effect, for scale
-    _, g_64 = O.loss_and_grads(P.astype(np.float64), xv, tgt, norm.astype(np.float64), w, emulate=False)
+    _, g_64 = O.loss_and_grads(P.astype(np.float64), xv, tgt, norm.astype(np.float64), w, emulate=False,
+                               huber=huber)
     assert np.linalg.norm(g - g_64) / np.linalg.norm(g_64) < 5e-2
 
 
@@ -164,6 +168,7 @@ def test_adam_step_matches_oracle(torch, searched):
 
 # ---- training and the gain over the plain fit ------------------------------------------------
 TRAIN_DB = dict(nproteins=3000, seed=21, nspec=3000, well_populated=2000)
+TAIL_HUBER = 0.5   # training loss: Huber's, delta 0.5 in normalised target units
 
 
 @pytest.fixture(scope="module")
@@ -188,15 +193,18 @@ def trained(torch):
                     np.isfinite(res["slope"]) & (res["slope"] < 0))[0]
     rng = np.random.default_rng(0)
     rng.shuffle(ok)
-    held, train = ok[:300], ok[300:]
+    held, calib, train = ok[:300], ok[300:600], ok[600:]
     m = T.TailModel(0, max_batch=8192, seed=11)
-    smp = T.plan(train, per_query=48, keep_range=(8, 512), seed=1)
+    m.set_loss(TAIL_HUBER)
+    smp = T.plan(train, per_query=64, keep_range=(8, 512), seed=1)
     x, t = T.training_set(m, dv, res, smp)
     m.set_norm_from(t.cpu().numpy())
-    losses = m.train(x, t, epochs=15, batch=512, opt=T.Adam(lr=1e-3), seed=2, lr_decay=0.85)
-    ev = T.evaluate(m, dv, res, T.plan(held, per_query=4, keep_range=(100, 500), seed=3))
-    return dict(model=m, losses=losses, eval=ev, n_train=len(smp), n_queries=len(ok), dev=dv, res=res, queries=q,
-                searcher=s)
+    losses = m.train(x, t, epochs=15, batch=512, opt=T.Adam(lr=1e-3, w_slope=0.2), seed=2, lr_decay=0.85)
+    cal = T.evaluate(m, dv, res, T.plan(calib, per_query=8, keep_range=(20, 500), seed=4))
+    below = T.choose_sparse_below(cal["err_plain"], cal["err_learned"], cal["cpsms_sub"])
+    ev = T.evaluate(m, dv, res, T.plan(held, per_query=8, keep_range=(20, 500), seed=3))
+    return dict(model=m, losses=losses, eval=ev, below=below, n_train=len(smp), n_queries=len(ok), dev=dv, res=res,
+                queries=q, searcher=s)
 
 
 def test_training_reduces_loss(trained):
@@ -205,23 +213,28 @@ def test_training_reduces_loss(trained):
 
 
 def test_learned_tail_beats_plain_fit_on_sparse_held_out(trained):
-    """Both lines against the plain fit of ALL the query's candidates, at the query's top
-    score.  That judge is itself unstable (refitting half of a query's own candidates moves
-    it by more than 1 log10 for most queries), so the gain is in the large errors: the
-    plain fit on 100-500 candidates extrapolates its steeper local slope far out."""
-    ev = trained["eval"]
-    ep, el = ev["err_plain"], ev["err_learned"]
+    """The fallback policy at its calibrated threshold, on held-out queries: well-populated
+    queries (not trained on, not calibrated on) subsampled to fewer candidates than the
+    threshold, each scored against the plain fit of ALL its candidates at the top score.
+    The learned line must beat the plain fit of the subsample on the median, the 90th and
+    the 99th percentile of |log10 e| error.  The judge is itself unstable (refitting half of
+    a query's own candidates moves it by more than 1 log10 for most queries), which bounds
+    how close either line can get."""
+    ev, below = trained["eval"], trained["below"]
+    assert below >= 50, below
+    m = ev["cpsms_sub"] < below
+    ep, el = ev["err_plain"][m], ev["err_learned"][m]
     q = lambda e, f: float(np.quantile(e, f))
     print(f"\n[tail] {trained['n_queries']} well-populated queries, {trained['n_train']} training samples; "
-          f"held-out {len(el)} subsamples of 100-500 candidates, |log10 e| error vs the full-data fit: "
-          f"mean plain {np.mean(np.minimum(ep, 1e3)):.2f} learned {np.mean(el):.2f}; "
-          f"median plain {q(ep, .5):.2f} learned {q(el, .5):.2f}; p90 plain {q(ep, .9):.2f} learned {q(el, .9):.2f}; "
-          f"p99 plain {q(ep, .99):.2f} learned {q(el, .99):.2f}; within 0.1: plain {np.mean(ep <= .1):.3f} "
-          f"learned {np.mean(el <= .1):.3f}; within 1: plain {np.mean(ep <= 1):.3f} learned {np.mean(el <= 1):.3f}")
+          f"threshold {below} candidates; held-out {len(el)} subsamples below it, |log10 e| error vs the full-data "
+          f"fit: median plain {q(ep, .5):.2f} learned {q(el, .5):.2f}; p90 plain {q(ep, .9):.2f} learned "
+          f"{q(el, .9):.2f}; p99 plain {q(ep, .99):.2f} learned {q(el, .99):.2f}; within 0.1: plain "
+          f"{np.mean(ep <= .1):.3f} learned {np.mean(el <= .1):.3f}")
+    assert len(el) >= 300
     assert np.all(np.isfinite(el))
-    assert np.mean(el) < np.mean(np.minimum(ep, 1e3))
-    assert q(el, 0.9) < 0.85 * q(ep, 0.9)
-    assert q(el, 0.99) < 0.85 * q(ep, 0.99)
+    assert q(el, 0.5) < q(ep, 0.5)
+    assert q(el, 0.9) < q(ep, 0.9)
+    assert q(el, 0.99) < q(ep, 0.99)
 
 
 def test_fallback_policy_on_search_results(torch, trained):
