@@ -379,6 +379,7 @@ def main():
     ap.add_argument("--spectra", type=int, default=0, help="search only the first N spectra (profiling cases)")
     ap.add_argument("--no-tail", action="store_true", help="leave the learned tail out of the step")
     ap.add_argument("--no-index-build", action="store_true", help="skip timing the GPU index build at set-up")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape")
     ap.add_argument("--sparse-below", type=int, default=0,
                     help="queries with fewer candidate PSMs take the learned tail (0: calibrated)")
     ap.add_argument("--tail-queries", type=int, default=16000,
@@ -517,6 +518,20 @@ def main():
             else:
                 tail = None
         log(f"[bench] learned tail: {tail_info}")
+
+    # ---- launch shape: the autotuner times every candidate on a seeded sample of the batch
+    tiles = None
+    if not args.plain and not args.no_autotune:
+        sel = np.sort(np.random.Generator(np.random.PCG64(9)).choice(q.n, size=min(q.n, 4096), replace=False))
+        tqd, tkeep = device_queries(q.subset(sel))
+        t0 = time.perf_counter()
+        tr = ws.autotune(tqd, params, reps=3, use_cache=False, stream=stream.cuda_stream)
+        tiles = {"chosen": tr["best"], "sample": int(len(sel)), "tune_s": round(time.perf_counter() - t0, 2),
+                 "candidates_ms": [[c["chunks_per_lane"], c["ctas_per_sm"], c["tile"], c["sorted"], round(c["ms"], 3)]
+                                   for c in tr["candidates"]],
+                 "candidate_fields": ["chunks_per_lane", "ctas_per_sm", "tile", "sorted", "ms"]}
+        log(f"[bench] autotuned launch shape: {tr['best']} ({tiles['tune_s']} s)")
+        del tqd, tkeep
 
     def step():
         ws.search_device(qd, params, t_out.data_ptr(), stream=stream.cuda_stream)
@@ -716,6 +731,7 @@ def main():
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback"},
             "kernel_ms": {k: v[1] / v[0] for k, v in kt.items()},
             "gpu_launches": launches,
+            "tiles": tiles if tiles else {"chosen": ws.tiles, "autotuned": False},
             "path": "plain" if args.plain else ("batched+learned tail" if tail else "batched"),
             "parity": parity,
             "index_build": index_build,

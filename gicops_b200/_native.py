@@ -105,6 +105,22 @@ class StreamStats(C.Structure):
                 ("search_ms", C.c_double), ("download_ms", C.c_double)]
 
 
+class Tiles(C.Structure):
+    _fields_ = [("chunks_per_lane", C.c_uint32), ("ctas_per_sm", C.c_uint32), ("tile", C.c_uint32),
+                ("sorted", C.c_uint32)]
+
+    def as_dict(self) -> dict:
+        return {f: int(getattr(self, f)) for f, _ in self._fields_}
+
+
+TUNE_MAX = 32
+
+
+class TuneResult(C.Structure):
+    _fields_ = [("best", Tiles), ("ncand", C.c_uint32), ("cached", C.c_uint32), ("cand", Tiles * TUNE_MAX),
+                ("ms", C.c_float * TUNE_MAX)]
+
+
 class TailAdam(C.Structure):
     _fields_ = [("lr", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float),
                 ("w_slope", C.c_float), ("w_lgs", C.c_float)]
@@ -138,6 +154,10 @@ _SIGS = [
                                         C.c_int32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("gx_workspace_create", C.c_int32, [C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(C.c_void_p)]),
     ("gx_workspace_free", C.c_int32, [C.c_void_p]),
+    ("gx_workspace_get_tiles", C.c_int32, [C.c_void_p, C.POINTER(Tiles)]),
+    ("gx_workspace_set_tiles", C.c_int32, [C.c_void_p, C.POINTER(Tiles)]),
+    ("gx_autotune", C.c_int32, [C.c_void_p, C.c_void_p, C.POINTER(Queries), C.POINTER(Params), C.c_uint32,
+                                C.c_uint32, C.POINTER(TuneResult), C.c_void_p]),
     ("gx_search_host", C.c_int32, [C.c_void_p, C.c_void_p, C.POINTER(Queries), C.POINTER(Params), C.c_void_p,
                                    C.c_void_p, C.c_void_p]),
     ("gx_search_device", C.c_int32, [C.c_void_p, C.c_void_p, C.POINTER(Queries), C.POINTER(Params), C.c_void_p,

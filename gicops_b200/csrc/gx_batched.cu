@@ -194,10 +194,9 @@ constexpr int kPend = GX_PEND;  // per-warp queue of candidates awaiting a hyper
 static_assert(kPend >= 128, "the queue must hold one scan step's candidates (32 lanes x 4)");
 constexpr int kIvlChunk = 256;  // intervals per span table
 constexpr int kDummy = 32;      // scorecard words that take the adds of ids outside the tile (one per lane)
-#ifndef GX_STREAM_CHUNKS
-#define GX_STREAM_CHUNKS 2
-#endif
-constexpr int kChunks = GX_STREAM_CHUNKS;   // 16-byte id chunks in flight per lane
+// 16-byte id chunks each lane loads per work unit before it scatters any: a template
+// parameter of the kernel (1..kMaxChunks), chosen per launch (BatchedTiles::chunks)
+constexpr int kMaxChunks = 3;
 constexpr int kHeapWarp = kBWarps - 1;      // inserts heap entrants while the others stream
 #ifndef GX_ENT_SMEM
 #define GX_ENT_SMEM 8
@@ -532,13 +531,14 @@ __device__ __forceinline__ void build_span_warp(BatchSmem &sm, const BatchDyn &d
 }
 
 // Stream the ids of every interval of the span table into the scorecard.  Warps take
-// units of 32 x kChunks consecutive 16-byte chunks (8 ids each) from a shared counter;
+// units of 32 x CH consecutive 16-byte chunks (8 ids each) from a shared counter;
 // lane l loads chunks l, l+32, ... of the unit, all before it scatters any.  The ids of
 // a chunk outside its interval (at most the first and last chunk of an interval have
 // some) are replaced through the keep masks: with the lane's dummy word when the tile
 // is a whole block (every id of the block is then a word of the tile and needs no
 // range check), else with 0xFFFF, which the range check sends to the dummy word
 // (0xFFFF - lo >= lim: lo + lim <= 2 * block entries < 0xFFFF).
+template <int CH>
 __device__ __forceinline__ void stream_tile(BatchSmem &sm, const BatchDyn &dd, const uint4 *__restrict__ ia4,
                                             uint32_t ncv, void *scv, int ctile, bool wide, bool whole, uint32_t lo,
                                             uint32_t lim, int lane)
@@ -551,7 +551,7 @@ __device__ __forceinline__ void stream_tile(BatchSmem &sm, const BatchDyn &dd, c
         uint32_t u = 0;
         if (lane == 0) u = atomicAdd(&sm.next_unit, 1u);
         u = __shfl_sync(0xffffffffu, u, 0);
-        const uint32_t j0 = u * (32u * kChunks);
+        const uint32_t j0 = u * (32u * CH);
         if (j0 >= M) break;
         // interval of the unit's first chunk (the last k < ncv with pre[k] <= j0, a non-empty
         // interval: pre is non-decreasing, pre[0] = 0 and pre[ncv] > j0); each lane walks on
@@ -571,10 +571,10 @@ __device__ __forceinline__ void stream_tile(BatchSmem &sm, const BatchDyn &dd, c
             if (dd.sp_pre[mid] <= j0) k = mid; else hi = mid;
         }
 #endif
-        uint4 v[kChunks];
-        uint32_t kx[kChunks];
+        uint4 v[CH];
+        uint32_t kx[CH];
 #pragma unroll
-        for (int p = 0; p < kChunks; p++) {
+        for (int p = 0; p < CH; p++) {
             const uint32_t j = j0 + (uint32_t)lane + 32u * p;
             kx[p] = 0xFFFFFFFFu;
             if (j < M) {
@@ -584,7 +584,7 @@ __device__ __forceinline__ void stream_tile(BatchSmem &sm, const BatchDyn &dd, c
             }
         }
 #pragma unroll
-        for (int p = 0; p < kChunks; p++) {
+        for (int p = 0; p < CH; p++) {
             if (kx[p] == 0xFFFFFFFFu) continue;
             const uint4 r = dd.sp_rec[kx[p]];
             const uint32_t j = j0 + (uint32_t)lane + 32u * p;
@@ -621,6 +621,7 @@ __device__ __forceinline__ void stream_tile(BatchSmem &sm, const BatchDyn &dd, c
     }
 }
 
+template <int CH>
 __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchArgs a)
 {
     extern __shared__ __align__(16) unsigned char dyn[];
@@ -757,7 +758,7 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
                                             a.spill_per_warp, a.heap_cap, lane);
                         heap_due = false;
                     }
-                    stream_tile(sm, dd, ia4, ncv, scv, ctile, wide, whole, lo, lim, lane);
+                    stream_tile<CH>(sm, dd, ia4, ncv, scv, ctile, wide, whole, lo, lim, lane);
                     if (ti == 0 && niA && tid < (int)nv) {   // the next tile's offsets, for its span table
                         dd.nx_s[tid] = nx_s;
                         dd.nx_e[tid] = nx_e;
@@ -948,11 +949,23 @@ cudaError_t fill_logtab(double *tab, uint32_t n, cudaStream_t st)
 
 size_t batched_dyn_smem(int tile) { return (size_t)tile * 8 + batch_dyn_bytes(tile); }
 
-// CTAs of k_search_batched that fit one SM at this tile size (at most kCtasPerSm).
-int batched_ctas_per_sm(int tile)
+namespace {
+using SearchKernel = void (*)(SearchArgs);
+SearchKernel search_kernel(int chunks)
+{
+    switch (chunks) {
+    case 1: return k_search_batched<1>;
+    case 3: return k_search_batched<3>;
+    default: return k_search_batched<2>;
+    }
+}
+}  // namespace
+
+// CTAs of k_search_batched<chunks> that fit one SM at this tile size (at most kCtasPerSm).
+int batched_ctas_per_sm(int tile, int chunks)
 {
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_search_batched, kBBlock, batched_dyn_smem(tile)) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, search_kernel(chunks), kBBlock, batched_dyn_smem(tile)) !=
         cudaSuccess)
         n = 1;
     return n < 1 ? 1 : (n > kCtasPerSm ? kCtasPerSm : n);
@@ -967,29 +980,43 @@ uint32_t batched_spill_per_warp(int tile)
 
 cudaError_t batched_set_attributes(int tile)
 {
-    return cudaFuncSetAttribute(k_search_batched, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)batched_dyn_smem(tile));
+    cudaError_t e = cudaSuccess;
+    for (int c = 1; c <= kMaxChunks && e == cudaSuccess; c++)
+        e = cudaFuncSetAttribute(search_kernel(c), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)batched_dyn_smem(tile));
+    return e;
 }
 
-cudaError_t launch_batched(SearchArgs a, const BatchedScratch &b, cudaStream_t st)
+bool batched_tiles_valid(const BatchedTiles &t, int max_tile)
+{
+    return t.chunks >= 1 && t.chunks <= kMaxChunks && t.ctas_per_sm >= 1 && t.ctas_per_sm <= kCtasPerSm &&
+           t.tile >= kMinTile && t.tile <= max_tile && t.tile % 32 == 0 && (t.sorted == 0 || t.sorted == 1);
+}
+
+cudaError_t launch_batched(SearchArgs a, const BatchedScratch &b, const BatchedTiles &t, cudaStream_t st)
 {
     cudaError_t e;
+    a.tile = t.tile;
     int h = prof_begin("k_prep", st);
     k_prep<<<a.nspec, kPrepBlock, 0, st>>>(a, const_cast<int2 *>(a.win), b.key_in, b.ord_in);
     prof_end(h, st);
     count_launch();
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    size_t tb = b.sort_temp_bytes;
-    h = prof_begin("sort_by_volume", st);
-    e = cub::DeviceRadixSort::SortPairsDescending(b.sort_temp, tb, b.key_in, b.key_out, b.ord_in, b.ord_out,
-                                                  (int)a.nspec, 0, 64, st);
-    prof_end(h, st);
-    count_launch();
-    if (e != cudaSuccess) return e;
+    a.order = b.ord_in;   // batch order
+    if (t.sorted) {       // heaviest scan volume first
+        size_t tb = b.sort_temp_bytes;
+        h = prof_begin("sort_by_volume", st);
+        e = cub::DeviceRadixSort::SortPairsDescending(b.sort_temp, tb, b.key_in, b.key_out, b.ord_in, b.ord_out,
+                                                      (int)a.nspec, 0, 64, st);
+        prof_end(h, st);
+        count_launch();
+        if (e != cudaSuccess) return e;
+        a.order = b.ord_out;
+    }
     if ((e = cudaMemsetAsync(a.queue, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
-    a.order = b.ord_out;
+    const int ctas = t.ctas_per_sm < b.max_ctas[t.chunks] ? t.ctas_per_sm : b.max_ctas[t.chunks];
     h = prof_begin("k_search_batched", st);
-    k_search_batched<<<b.grid, kBBlock, batched_dyn_smem(a.tile), st>>>(a);
+    search_kernel(t.chunks)<<<b.sms * ctas, kBBlock, batched_dyn_smem(a.tile), st>>>(a);
     prof_end(h, st);
     count_launch();
     if ((e = cudaGetLastError()) != cudaSuccess) return e;

@@ -15,16 +15,27 @@ struct BatchedScratch {
     uint32_t *ord_in, *ord_out;   // spectrum ids
     void *sort_temp;
     size_t sort_temp_bytes;
-    int grid;                     // persistent CTAs
+    int sms;                      // SMs of the device
+    int max_ctas[4];              // resident CTAs per SM of k_search_batched<c>, c = 1..3
 };
+
+// Launch shape of the batched path, chosen per workspace (gx_tiles of the C ABI).
+struct BatchedTiles {
+    int chunks = 2;               // 16-byte id chunks per lane per work unit, 1..3
+    int ctas_per_sm = 2;          // persistent CTAs per SM, 1..2 (at most what fits)
+    int tile = 0;                 // candidates per scorecard tile (0: the index's block)
+    int sorted = 1;               // 1: spectra heaviest first; 0: batch order
+};
+constexpr int kMinTile = 1024;
 
 size_t batched_sort_temp_bytes(uint32_t max_spec);
 // log10(x) for x in [0, n), computed on the device by the function the kernels call
 cudaError_t fill_logtab(double *tab, uint32_t n, cudaStream_t st);
 constexpr uint32_t kLogTab = 1u << 20;
 cudaError_t batched_set_attributes(int tile);
-int batched_ctas_per_sm(int tile);   // after batched_set_attributes
+int batched_ctas_per_sm(int tile, int chunks);   // after batched_set_attributes
 uint32_t batched_spill_per_warp(int tile);
-cudaError_t launch_batched(SearchArgs a, const BatchedScratch &b, cudaStream_t st);
+bool batched_tiles_valid(const BatchedTiles &t, int max_tile);
+cudaError_t launch_batched(SearchArgs a, const BatchedScratch &b, const BatchedTiles &t, cudaStream_t st);
 
 }  // namespace gx

@@ -10,11 +10,14 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/gicops_b200.h"
@@ -397,7 +400,8 @@ struct gx_workspace {
     uint32_t spill_per_warp = 0;
     double *logtab = nullptr;
     BatchedScratch bs{};
-    int tile = kBlockEntries;
+    int tile = kBlockEntries;   // largest candidate tile the buffers hold (the index's block)
+    BatchedTiles tiles{};       // launch shape of the batched path (gx_workspace_set_tiles, gx_autotune)
 };
 
 extern "C" const char *gx_last_error(void) { return g_last_error.c_str(); }
@@ -511,10 +515,13 @@ extern "C" gx_status gx_workspace_create(const gx_index *ix, uint32_t max_spec, 
         cudaGetDevice(&dev);
         e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (e == cudaSuccess) e = batched_set_attributes(ws->tile);
-        ws->bs.grid = sms * batched_ctas_per_sm(ws->tile);
+        ws->bs.sms = sms;
+        for (int c = 1; c <= 3; c++) ws->bs.max_ctas[c] = batched_ctas_per_sm(ws->tile, c);
     }
+    ws->tiles.tile = ws->tile;
     ws->spill_per_warp = batched_spill_per_warp(ws->tile);
-    al((void **)&ws->spill, sizeof(Cell) * (uint64_t)ws->bs.grid * 32 * ws->spill_per_warp);
+    // entrant spill of every warp of the largest grid (two CTAs of 16 warps per SM)
+    al((void **)&ws->spill, sizeof(Cell) * (uint64_t)ws->bs.sms * 32 * ws->spill_per_warp);
     al((void **)&ws->logtab, sizeof(double) * kLogTab);
     if (e == cudaSuccess) e = fill_logtab(ws->logtab, kLogTab, nullptr);
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
@@ -585,12 +592,11 @@ gx_status launch_search(gx_index *ix, gx_workspace *ws, const gx_queries *q, con
         if (q->npeaks > ws->max_peaks) return fail(GX_ERR_INVLD_SIZE, "more peaks than the workspace holds");
         a.ivl = ws->ivl; a.ivl_cap = 2ull * ws->max_peaks; a.nivl = ws->nivl; a.guard = ws->guard; a.queue = ws->queue;
         a.hist_g = hist ? hist : ws->hist_g;
-        a.tile = ws->tile;
         a.spill = ws->spill;
         a.logtab = ws->logtab;
         a.logtab_n = kLogTab;
         a.spill_per_warp = ws->spill_per_warp;
-        cudaError_t e = launch_batched(a, ws->bs, st);
+        cudaError_t e = launch_batched(a, ws->bs, ws->tiles, st);
         if (e != cudaSuccess) return cuda_fail(e, "batched search launch");
         if (ws->tail && ws->tail_below)
             return gx_tail_apply(ws->tail, a.hist_g, out, q->prec, q->charge, q->nspec, ws->tail_below, p->expect_max,
@@ -629,6 +635,148 @@ extern "C" gx_status gx_workspace_set_tail(gx_workspace *ws, gx_tail_model *m, u
     if (!ws) return fail(GX_ERR_INVLD_PTR, "gx_workspace_set_tail: null workspace");
     ws->tail = m;
     ws->tail_below = m ? sparse_below : 0u;
+    return GX_SUCCESS;
+}
+
+// ---- launch shape and its autotuner -------------------------------------------------------
+namespace {
+
+gx_tiles to_c(const BatchedTiles &t)
+{
+    return gx_tiles{(uint32_t)t.chunks, (uint32_t)t.ctas_per_sm, (uint32_t)t.tile, (uint32_t)t.sorted};
+}
+
+BatchedTiles from_c(const gx_tiles &t)
+{
+    BatchedTiles b;
+    b.chunks = (int)t.chunks_per_lane;
+    b.ctas_per_sm = (int)t.ctas_per_sm;
+    b.tile = (int)t.tile;
+    b.sorted = (int)t.sorted;
+    return b;
+}
+
+// Workload shape the autotuner's choice is cached for: the index, and the parameters that
+// decide the candidate windows and the scoring work of a spectrum.
+struct TuneKey {
+    const gx_index *ix;
+    uint64_t dM_bits;   // the batch's tolerance (Da) bits; ~0 with per-spectrum tolerances
+    uint32_t dF, min_shp, cap, flags, maxz;
+    bool operator<(const TuneKey &o) const
+    {
+        return std::tie(ix, dM_bits, dF, min_shp, cap, flags, maxz) <
+               std::tie(o.ix, o.dM_bits, o.dF, o.min_shp, o.cap, o.flags, o.maxz);
+    }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, BatchedTiles> g_tune_cache;
+
+}  // namespace
+
+extern "C" gx_status gx_workspace_get_tiles(const gx_workspace *ws, gx_tiles *t)
+{
+    if (!ws || !t) return fail(GX_ERR_INVLD_PTR, "gx_workspace_get_tiles: null argument");
+    *t = to_c(ws->tiles);
+    return GX_SUCCESS;
+}
+
+extern "C" gx_status gx_workspace_set_tiles(gx_workspace *ws, const gx_tiles *t)
+{
+    if (!ws || !t) return fail(GX_ERR_INVLD_PTR, "gx_workspace_set_tiles: null argument");
+    const BatchedTiles b = from_c(*t);
+    if (!batched_tiles_valid(b, ws->tile))
+        return fail(GX_ERR_INVLD_PARAM, "gx_workspace_set_tiles: chunks_per_lane 1..3, ctas_per_sm 1..2, tile a "
+                                        "multiple of 32 in 1024.." + std::to_string(ws->tile) + ", sorted 0 or 1");
+    ws->tiles = b;
+    return GX_SUCCESS;
+}
+
+extern "C" gx_status gx_autotune(gx_index *ix, gx_workspace *ws, const gx_queries *q, const gx_params *p, uint32_t reps,
+                                 uint32_t use_cache, gx_tune_result *out, void *stream)
+{
+    if (!ix || !ws || !q || !p || !out) return fail(GX_ERR_INVLD_PTR, "gx_autotune: null argument");
+    if (ws->ix != ix) return fail(GX_ERR_INVLD_PARAM, "gx_autotune: workspace belongs to another index");
+    if (p->flags & GX_FLAG_PLAIN) return fail(GX_ERR_INVLD_PARAM, "gx_autotune: the plain path has no tiles to tune");
+    if (q->nspec == 0) return fail(GX_ERR_INVLD_SIZE, "gx_autotune: an empty sample");
+    int32_t cap;
+    gx_status rc = check_params(ix, p, &cap);
+    if (rc != GX_SUCCESS) return rc;
+    std::memset(out, 0, sizeof(*out));
+    TuneKey key{ix, 0, p->dF, p->min_shp, (uint32_t)cap, p->flags, ix->maxz};
+    if (q->dM) key.dM_bits = ~0ull;
+    else std::memcpy(&key.dM_bits, &p->dM, sizeof(double));
+    if (use_cache) {
+        std::lock_guard<std::mutex> g(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end() && batched_tiles_valid(it->second, ws->tile)) {
+            ws->tiles = it->second;
+            out->best = to_c(it->second);
+            out->cached = 1;
+            return GX_SUCCESS;
+        }
+    }
+    DeviceScope ds(ix->device);
+    GX_CUDA(ds.status());
+    cudaStream_t st = (cudaStream_t)stream;
+    if (reps == 0) reps = 1;
+    // candidates: id chunks per lane x CTAs per SM x tile width x spectrum order
+    std::vector<BatchedTiles> cand;
+    const int tiles[2] = {ws->tile, (ws->tile * 3 / 4) & ~31};
+    for (int c = 1; c <= 3; c++)
+        for (int k = 1; k <= 2; k++)
+            for (int ti = 0; ti < 2; ti++)
+                for (int so = 1; so >= 0; so--) {
+                    BatchedTiles b;
+                    b.chunks = c;
+                    b.ctas_per_sm = k;
+                    b.tile = tiles[ti];
+                    b.sorted = so;
+                    if (k <= ws->bs.max_ctas[c] && batched_tiles_valid(b, ws->tile) && cand.size() < GX_TUNE_MAX)
+                        cand.push_back(b);
+                }
+    const BatchedTiles keep = ws->tiles;
+    std::vector<cudaEvent_t> ev(reps + 1);
+    for (auto &e : ev) GX_CUDA(cudaEventCreate(&e));
+    auto cleanup = [&]() {
+        for (auto &e : ev) cudaEventDestroy(e);
+    };
+    float best_ms = INFINITY;
+    BatchedTiles best = keep;
+    for (size_t i = 0; i < cand.size(); i++) {
+        ws->tiles = cand[i];
+        rc = launch_search(ix, ws, q, p, ws->out, nullptr, nullptr, st);   // warm-up
+        std::vector<float> t(reps);
+        for (uint32_t r = 0; r < reps && rc == GX_SUCCESS; r++) {
+            cudaEventRecord(ev[r], st);
+            rc = launch_search(ix, ws, q, p, ws->out, nullptr, nullptr, st);
+            cudaEventRecord(ev[r + 1], st);
+        }
+        cudaError_t e = cudaStreamSynchronize(st);
+        if (rc != GX_SUCCESS || e != cudaSuccess) {
+            ws->tiles = keep;
+            cleanup();
+            return rc != GX_SUCCESS ? rc : cuda_fail(e, "gx_autotune");
+        }
+        // back-to-back launches: each one's time is the gap between its two events
+        for (uint32_t r = 0; r < reps; r++) cudaEventElapsedTime(&t[r], ev[r], ev[r + 1]);
+        std::sort(t.begin(), t.end());
+        const float ms = t[reps / 2];
+        out->cand[i] = to_c(cand[i]);
+        out->ms[i] = ms;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = cand[i];
+        }
+    }
+    cleanup();
+    out->ncand = (uint32_t)cand.size();
+    out->best = to_c(best);
+    ws->tiles = best;
+    {
+        std::lock_guard<std::mutex> g(g_tune_mu);
+        g_tune_cache[key] = best;
+    }
+    cudaGetLastError();
     return GX_SUCCESS;
 }
 

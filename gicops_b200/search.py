@@ -82,6 +82,31 @@ class Searcher:
         N.check(N.lib().gx_workspace_set_tail(self.handle, model.handle if model else None, sparse_below))
         self._tail = model   # keep the model alive while attached
 
+    @property
+    def tiles(self) -> dict:
+        """Launch shape of the batched path (gx_tiles)."""
+        t = N.Tiles()
+        N.check(N.lib().gx_workspace_get_tiles(self.handle, C.byref(t)))
+        return t.as_dict()
+
+    @tiles.setter
+    def tiles(self, t: dict) -> None:
+        c = N.Tiles(t["chunks_per_lane"], t["ctas_per_sm"], t["tile"], t["sorted"])
+        N.check(N.lib().gx_workspace_set_tiles(self.handle, C.byref(c)))
+
+    def autotune(self, q_dev: dict, params: SearchParams, reps: int = 3, use_cache: bool = True,
+                 stream: int = 0) -> dict:
+        """Time every launch shape on a device-resident sample of the workload (gx_autotune),
+        keep the fastest on this workspace; returns the choice and every candidate's time."""
+        cq = N.Queries(q_dev["nspec"], q_dev["npeaks"], q_dev["idx"], q_dev["moz"], q_dev["intn"], q_dev["prec"],
+                       q_dev.get("charge"), q_dev.get("dM"))
+        p = params.c()
+        r = N.TuneResult()
+        N.check(N.lib().gx_autotune(self.index.handle, self.handle, C.byref(cq), C.byref(p), reps, int(use_cache),
+                                    C.byref(r), stream))
+        return {"best": r.best.as_dict(), "cached": bool(r.cached),
+                "candidates": [dict(r.cand[i].as_dict(), ms=float(r.ms[i])) for i in range(r.ncand)]}
+
     def search(self, q: QueryBatch, params: SearchParams, heap: bool = False, hist: bool = False) -> SearchResults:
         """Host buffers in, host results out (H2D, kernels, D2H, synchronise)."""
         n = q.n

@@ -248,6 +248,40 @@ gx_status gx_merge_shards_device(uint32_t nspec, int32_t world, uint32_t k, cons
 gx_status gx_workspace_create(const gx_index *ix, uint32_t max_spec, uint32_t max_peaks, gx_workspace **out);
 gx_status gx_workspace_free(gx_workspace *ws);
 
+/* ---- launch shape of the batched path and its autotuner (no counterpart in the
+ * reference, whose launch shape is fixed: superstep3/kernel.cu:588-598) ---------------
+ * chunks_per_lane: 16-byte id chunks (8 ids) each lane loads per work unit (the bucket
+ * chunk), 1..3; ctas_per_sm: persistent CTAs per SM, each on its own spectrum, 1..2;
+ * tile: candidates per shared-memory scorecard tile (the scorecard partition width), a
+ * multiple of 32 from 1024 to the index's block of 11,264 entries; sorted: 1 takes the
+ * spectra heaviest first (a sort by scan volume), 0 in batch order.  Results do not
+ * depend on the shape.  A new workspace starts at {2, 2, 11264, 1}. */
+typedef struct {
+    uint32_t chunks_per_lane;
+    uint32_t ctas_per_sm;
+    uint32_t tile;
+    uint32_t sorted;
+} gx_tiles;
+gx_status gx_workspace_get_tiles(const gx_workspace *ws, gx_tiles *t);
+gx_status gx_workspace_set_tiles(gx_workspace *ws, const gx_tiles *t);
+#define GX_TUNE_MAX 32
+typedef struct {
+    gx_tiles best;
+    uint32_t ncand;               /* candidates timed (0 when taken from the cache) */
+    uint32_t cached;              /* 1: an earlier call's choice for the same workload shape */
+    gx_tiles cand[GX_TUNE_MAX];
+    float ms[GX_TUNE_MAX];        /* median of `reps` timed searches of the sample, per candidate */
+} gx_tune_result;
+/* Times every candidate shape (chunks 1-3 x CTAs per SM 1-2 x tile {block, 3/4 block} x
+ * sorted or not) on the sample q_dev (device buffers: a few thousand spectra of the
+ * workload), one warm-up and `reps` timed searches each on `stream`, sets the fastest on
+ * the workspace and caches it for the workload shape (index, tolerance or per-spectrum
+ * tolerances, dF, min_shp, heap capacity, flags, maxz).  With use_cache, a cached choice
+ * for the same shape is set without timing anything.  Synchronises the stream; writes
+ * the workspace's own result buffer only. */
+gx_status gx_autotune(gx_index *ix, gx_workspace *ws, const gx_queries *q_dev, const gx_params *p, uint32_t reps,
+                      uint32_t use_cache, gx_tune_result *out, void *stream);
+
 /* Search with HOST buffers (the drop-in for s3::search + s4::processResults):
  * copies queries in, runs the path, copies results out, synchronises.
  * heap_out (optional): [nspec * cap] final heap arrays; hist_out (optional):
