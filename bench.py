@@ -62,6 +62,13 @@ WORKLOADS = {
 }
 
 
+# The stress configuration: 1M proteins with Met oxidation <= 3 (about 200M index entries and
+# 16G fragment-ion ids, built on the GPU), 1M spectra at +-500 Da streamed from pinned host
+# memory in 64k-spectrum chunks (--stream-run; a measurement beside the bench, not its step)
+STRESS = dict(nproteins=1000000, db_seed=1, maxz=2, mods=[("M", 15.9949, 3)], nmods=3, nspec=1000000, dM=500.0,
+              chunk=65536, q=dict(charges=(2, 4), frag_charge2=True, keep_p=(0.2, 0.8), noise_mode="fill",
+                                  npeaks_range=(30, 150)))
+
 # spectra per step of the reference's CPU path: a seeded random subset of the workload's
 # batch (the whole batch where it takes seconds), sized for a few seconds per step
 REF_SAMPLE = {"large-200k": 1024, "mixed-20k": 4096, "open-20k": 2048, "closed-1k": 2000}
@@ -284,6 +291,143 @@ def reference_cpu(w: dict, db, q, sel, steps: int, warmup: int):
     return dict(value=sample / per, cores=cores, sample=sample, seconds=per, steps=len(each))
 
 
+def train_tail(ws, qd, params, t_out, t_hist, t_pre, t_chg, device: int, n_train: int, sparse_below: int):
+    """The learned tail, trained (untimed) on the batch's own well-populated queries (+-500 Da,
+    at least 10^4 candidates): 64 subsamples of each one's histogram against the plain fit of
+    all its candidates, with Huber's loss.  The candidate threshold below which the model
+    replaces the plain fit is calibrated on 300 other such queries (unless given), and the
+    gain reported on 300 held-out ones.  Returns (model or None, info dict)."""
+    import torch
+    import gicops_b200._native as N
+    import gicops_b200.tail as T
+    t0 = time.perf_counter()
+    stream = torch.cuda.current_stream()
+    ws.search_device(qd, params, t_out.data_ptr(), hist_dev=t_hist.data_ptr(), stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    res0 = t_out.cpu().numpy().view(N.RESULT_DTYPE)
+    pop = np.nonzero(((res0["status"] & 1) != 0) & (res0["cpsms"] >= 10000) & np.isfinite(res0["slope"]) &
+                     (res0["slope"] < 0))[0]
+    pop = np.random.default_rng(7).permutation(pop)
+    held, calib, train = pop[:300], pop[300:600], pop[600:600 + n_train]
+    if len(train) < 64:
+        return None, {"skipped": f"{len(pop)} well-populated queries"}
+    tail = T.TailModel(device, max_batch=8192, seed=11)
+    tail.set_loss(0.5)
+    dv = dict(hist=t_hist, res=t_out, prec=t_pre, charge=t_chg)
+    smp = T.plan(train, per_query=64, keep_range=(8, 512), seed=1)
+    xs, ts = T.training_set(tail, dv, res0, smp)
+    tail.set_norm_from(ts.cpu().numpy())
+    losses = tail.train(xs, ts, epochs=6, batch=512, opt=T.Adam(lr=1e-3, w_slope=0.2), seed=2, lr_decay=0.8)
+    del xs, ts
+    cal = T.evaluate(tail, dv, res0, T.plan(calib, per_query=8, keep_range=(20, 500), seed=4))
+    below = sparse_below or T.choose_sparse_below(cal["err_plain"], cal["err_learned"], cal["cpsms_sub"])
+    ev = T.evaluate(tail, dv, res0, T.plan(held, per_query=8, keep_range=(20, 500), seed=3))
+    m = ev["cpsms_sub"] < below
+    qf = lambda e, f: round(float(np.quantile(e, f)), 3) if len(e) else None  # noqa: E731
+    ep, el = ev["err_plain"][m], ev["err_learned"][m]
+    info = {"sparse_below": int(below), "sparse_below_from": "argument" if sparse_below else
+            "calibration (300 held-out well-populated queries subsampled to 20-500 candidates)",
+            "loss": "huber 0.5", "train_queries": int(len(train)), "train_samples": int(len(smp)),
+            "train_loss": [round(x, 4) for x in losses], "train_s": round(time.perf_counter() - t0, 2),
+            "held_out": {"queries": int(len(held)), "subsamples_below_threshold": int(m.sum()),
+                         "abs_log10_e_error_vs_full_fit": {
+                             "plain": {"median": qf(ep, .5), "p90": qf(ep, .9), "p99": qf(ep, .99)},
+                             "learned": {"median": qf(el, .5), "p90": qf(el, .9), "p99": qf(el, .99)}},
+                         "share_within_0.1_log10": {"plain": float(np.mean(ep <= .1)) if len(ep) else None,
+                                                    "learned": float(np.mean(el <= .1)) if len(el) else None}}}
+    log(f"[bench] learned tail: {info}")
+    return (tail if below > 0 else None), info
+
+
+_STRESS_ENTRIES = None
+
+
+def _stress_part(n: int, seed: int, qargs: dict):
+    from gicops_b200 import synth
+    return synth.make_queries(_STRESS_ENTRIES, n, seed=seed, **qargs)
+
+
+def stream_run(args) -> None:
+    """The stress configuration through the streamed entry point: index entries on the host,
+    fragment ions, CSR and block layout on the GPU (gx_index_build); 1M spectra, drawn in
+    64k-spectrum parts by forked workers before CUDA starts, searched from pinned host memory
+    by gx_search_stream with the learned tail attached (trained on the first chunk).  Prints
+    one JSON line: spectra/s over the whole streamed batch (GPU clock, first upload to last
+    download) and the share of the copies hidden behind the search."""
+    global _STRESS_ENTRIES
+    import multiprocessing as mp
+    import gicops_b200 as gx
+    w = STRESS
+    t0 = time.time()
+    db = gx.synth.make_database(w["nproteins"], seed=w["db_seed"])
+    t1 = time.perf_counter()
+    E = gx.HostIndex.build(db, maxz=w["maxz"], mods=w["mods"], nmods=w["nmods"], ions=False)
+    entries_s = time.perf_counter() - t1
+    del db
+    _STRESS_ENTRIES = E.entries_by_len()
+    nspec = args.stream_spectra or w["nspec"]
+    parts = [(min(w["chunk"], nspec - i), 5000 + k) for k, i in enumerate(range(0, nspec, w["chunk"]))]
+    with mp.get_context("fork").Pool(min(len(parts), os.cpu_count() or 1)) as pool:   # before any CUDA call
+        q = gx.synth.QueryBatch.concat(pool.starmap(_stress_part, [(n, sd, w["q"]) for n, sd in parts]))
+    log(f"[stress] {E.total_entries()} entries, {q.n} spectra, {len(q.moz)} peaks ({time.time() - t0:.1f}s)")
+
+    import torch
+    import gicops_b200._native as N
+    torch.cuda.set_device(0)
+    d = torch.device("cuda", 0)
+    t1 = time.perf_counter()
+    dev = gx.DeviceIndex(E, 0)
+    torch.cuda.synchronize()
+    build_s = time.perf_counter() - t1
+    log(f"[stress] device index {dev.nbytes / 1e9:.1f} GB built in {build_s:.1f}s")
+    params = gx.SearchParams(dM=w["dM"], dF=5, topmatches=5, expect_max=20.0)
+    tail = tail_info = None
+    if not args.no_tail:
+        q0 = q.subset(np.arange(min(w["chunk"], q.n)))
+        ws0 = gx.Searcher(dev, q0.n, len(q0.moz))
+        t = {k: torch.from_numpy(np.ascontiguousarray(v)).to(d) for k, v in
+             dict(idx=q0.idx.view(np.int32), moz=q0.moz, intn=q0.intn, prec=q0.prec,
+                  charge=q0.charge.astype(np.int32)).items()}
+        qd0 = dict(nspec=q0.n, npeaks=len(q0.moz), **{k: v.data_ptr() for k, v in t.items()})
+        out0 = torch.empty(q0.n * N.RESULT_DTYPE.itemsize, dtype=torch.uint8, device=d)
+        hist0 = torch.empty((q0.n, N.HIST_BINS), dtype=torch.int32, device=d)
+        tail, tail_info = train_tail(ws0, qd0, params, out0, hist0, t["prec"], t["charge"], 0, args.tail_queries,
+                                     args.sparse_below)
+        del ws0, out0, hist0, t
+    st = gx.Streamer(dev, chunk=w["chunk"])
+    if tail is not None:
+        st.set_tail(tail, tail_info["sparse_below"])
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    qp = gx.synth.QueryBatch(pin(q.idx), pin(q.moz), pin(q.intn), pin(q.prec), pin(q.charge.astype(np.int32)),
+                             q.rtime)
+    out = torch.empty(q.n * N.RESULT_DTYPE.itemsize, dtype=torch.uint8).pin_memory().numpy().view(N.RESULT_DTYPE)
+    st.search(qp.subset(np.arange(min(2 * w["chunk"], q.n))), params)          # warm-up: two chunks
+    clocks, stop = [], threading.Event()
+    th = threading.Thread(target=sample_clocks, args=(stop, clocks, 0), daemon=True)
+    th.start()
+    time.sleep(0.5)
+    t1 = time.perf_counter()
+    res, stats = st.search(qp, params, out=out, stats=True)
+    wall = time.perf_counter() - t1
+    stop.set()
+    th.join(timeout=5)
+    copies = stats["upload_ms"] + stats["download_ms"]
+    hidden = stats["upload_ms"] + stats["search_ms"] + stats["download_ms"] - stats["total_ms"]
+    line = {"metric": "streamed query spectra/s (stress configuration)", "value": q.n / (stats["total_ms"] / 1e3),
+            "unit": "spectra/s", "n_gpus": 1, "wall_s": round(wall, 2), "host_wall_spectra_per_s": q.n / wall,
+            "stream": {k: (round(v, 2) if isinstance(v, float) else v) for k, v in stats.items()},
+            "copies_hidden_share": round(max(0.0, min(1.0, hidden / copies)), 3) if copies > 0 else None,
+            "search_share_of_total": round(stats["search_ms"] / stats["total_ms"], 3),
+            "config": {"proteins": w["nproteins"], "index_entries": E.total_entries(), "spectra": q.n,
+                       "chunk": w["chunk"], "window_da": w["dM"], "index_gb": round(dev.nbytes / 1e9, 1),
+                       "entries_s": round(entries_s, 1), "device_build_s": round(build_s, 1)},
+            "learned_tail": dict(tail_info or {}, queries_replaced=int(
+                ((res["status"] & N.STATUS_LEARNED_TAIL) != 0).sum())) if tail is not None else tail_info,
+            "reported_psms": int(((res["status"] & 2) != 0).sum()),
+            "clocks": summarize_clocks(clocks)}
+    print(json.dumps(line), flush=True)
+
+
 def parity_block(gx, N, H, q, params, w, run_full, tail_on: bool, n_sample: int = 256, n_hyp: int = 32) -> dict:
     """Untimed check of the benchmarked batch's own outputs: one more search of the whole
     batch (the timed step's launch sequence, with heap and histogram outputs) against the
@@ -384,8 +528,14 @@ def main():
                     help="queries with fewer candidate PSMs take the learned tail (0: calibrated)")
     ap.add_argument("--tail-queries", type=int, default=16000,
                     help="well-populated queries the learned tail is trained on (64 subsamples each)")
+    ap.add_argument("--stream-run", action="store_true",
+                    help="the stress configuration streamed through gx_search_stream (its own JSON line)")
+    ap.add_argument("--stream-spectra", type=int, default=0, help="spectra of the stress run (0: 1M)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.stream_run:
+        stream_run(args)
+        return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -472,52 +622,14 @@ def main():
     t_out = torch.empty(q.n * N.RESULT_DTYPE.itemsize, dtype=torch.uint8, device=d)
     t_hist = torch.empty((q.n, N.HIST_BINS), dtype=torch.int32, device=d)
 
-    # ---- learned tail: trained here (untimed) on this workload's well-populated queries:
-    # subsamples of their histograms against the plain fit of all their candidates; the
-    # candidate threshold below which the model replaces the plain fit is calibrated on
-    # other such queries, and the gain reported on a third, held-out set ------------------
+    # ---- learned tail: trained here (untimed) on this workload's well-populated queries --
     tail = None
     tail_info = None
     if not args.no_tail and not args.plain:
-        import gicops_b200.tail as T
-        t0 = time.perf_counter()
-        ws.search_device(qd, params, t_out.data_ptr(), hist_dev=t_hist.data_ptr(), stream=stream.cuda_stream)
-        torch.cuda.synchronize()
-        res0 = t_out.cpu().numpy().view(N.RESULT_DTYPE)
-        pop = np.nonzero(((res0["status"] & 1) != 0) & (res0["cpsms"] >= 10000) & np.isfinite(res0["slope"]) &
-                         (res0["slope"] < 0))[0]
-        pop = np.random.default_rng(7).permutation(pop)
-        held, calib, train = pop[:300], pop[300:600], pop[600:600 + args.tail_queries]
-        if len(train) >= 64:
-            tail = T.TailModel(local, max_batch=8192, seed=11)
-            tail.set_loss(0.5)
-            dv = dict(hist=t_hist, res=t_out, prec=t_pre, charge=t_chg)
-            smp = T.plan(train, per_query=64, keep_range=(8, 512), seed=1)
-            xs, ts = T.training_set(tail, dv, res0, smp)
-            tail.set_norm_from(ts.cpu().numpy())
-            losses = tail.train(xs, ts, epochs=6, batch=512, opt=T.Adam(lr=1e-3, w_slope=0.2), seed=2, lr_decay=0.8)
-            del xs, ts
-            cal = T.evaluate(tail, dv, res0, T.plan(calib, per_query=8, keep_range=(20, 500), seed=4))
-            below = args.sparse_below or T.choose_sparse_below(cal["err_plain"], cal["err_learned"], cal["cpsms_sub"])
-            ev = T.evaluate(tail, dv, res0, T.plan(held, per_query=8, keep_range=(20, 500), seed=3))
-            m = ev["cpsms_sub"] < below
-            qf = lambda e, f: round(float(np.quantile(e, f)), 3) if len(e) else None  # noqa: E731
-            ep, el = ev["err_plain"][m], ev["err_learned"][m]
-            tail_info = {"sparse_below": int(below), "sparse_below_from": "argument" if args.sparse_below else
-                         "calibration (300 held-out well-populated queries subsampled to 20-500 candidates)",
-                         "loss": "huber 0.5", "train_queries": int(len(train)), "train_samples": int(len(smp)),
-                         "train_loss": [round(x, 4) for x in losses], "train_s": round(time.perf_counter() - t0, 2),
-                         "held_out": {"queries": int(len(held)), "subsamples_below_threshold": int(m.sum()),
-                                      "abs_log10_e_error_vs_full_fit": {
-                                          "plain": {"median": qf(ep, .5), "p90": qf(ep, .9), "p99": qf(ep, .99)},
-                                          "learned": {"median": qf(el, .5), "p90": qf(el, .9), "p99": qf(el, .99)}},
-                                      "share_within_0.1_log10": {"plain": float(np.mean(ep <= .1)) if len(ep) else None,
-                                                                 "learned": float(np.mean(el <= .1)) if len(el) else None}}}
-            if below > 0:
-                ws.set_tail(tail, below)   # every search below applies it after the plain fit
-            else:
-                tail = None
-        log(f"[bench] learned tail: {tail_info}")
+        tail, tail_info = train_tail(ws, qd, params, t_out, t_hist, t_pre, t_chg, local, args.tail_queries,
+                                     args.sparse_below)
+        if tail is not None:
+            ws.set_tail(tail, tail_info["sparse_below"])   # every search below applies it after the plain fit
 
     # ---- launch shape: the autotuner times every candidate on a seeded sample of the batch
     tiles = None

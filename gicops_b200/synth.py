@@ -179,6 +179,25 @@ class QueryBatch:
                           self.rtime[sel], None if self.dM is None else self.dM[sel],
                           None if self.truth is None else self.truth[sel])
 
+    @staticmethod
+    def concat(batches) -> "QueryBatch":
+        """One batch of the spectra of several, in order."""
+        idx = [np.zeros(1, np.int64)]
+        off = 0
+        for b in batches:
+            idx.append(b.idx[1:].astype(np.int64) + off)
+            off += int(b.idx[-1])
+        dm = None
+        if any(b.dM is not None for b in batches):
+            dm = np.concatenate([b.dM if b.dM is not None else np.full(b.n, np.nan) for b in batches])
+        truth = None
+        if all(b.truth is not None for b in batches):
+            truth = np.concatenate([b.truth for b in batches])
+        return QueryBatch(np.concatenate(idx).astype(np.uint32), np.concatenate([b.moz for b in batches]),
+                          np.concatenate([b.intn for b in batches]), np.concatenate([b.prec for b in batches]),
+                          np.concatenate([b.charge for b in batches]), np.concatenate([b.rtime for b in batches]),
+                          dm, truth)
+
     def write_pbin(self, path: str) -> None:
         with open(path, "wb") as f:
             for i in range(self.n):
