@@ -524,6 +524,7 @@ def main():
     ap.add_argument("--no-tail", action="store_true", help="leave the learned tail out of the step")
     ap.add_argument("--no-index-build", action="store_true", help="skip timing the GPU index build at set-up")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape")
+    ap.add_argument("--no-graph", action="store_true", help="launch the step's kernels directly (no CUDA graph)")
     ap.add_argument("--sparse-below", type=int, default=0,
                     help="queries with fewer candidate PSMs take the learned tail (0: calibrated)")
     ap.add_argument("--tail-queries", type=int, default=16000,
@@ -644,6 +645,11 @@ def main():
                  "candidate_fields": ["chunks_per_lane", "ctas_per_sm", "tile", "sorted", "ms"]}
         log(f"[bench] autotuned launch shape: {tr['best']} ({tiles['tune_s']} s)")
         del tqd, tkeep
+
+    # the step's launch sequence is captured once in a CUDA graph and replayed
+    use_graph = not args.plain and not args.no_graph
+    if use_graph:
+        ws.set_graph(True)
 
     def step():
         ws.search_device(qd, params, t_out.data_ptr(), stream=stream.cuda_stream)
@@ -843,6 +849,7 @@ def main():
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback"},
             "kernel_ms": {k: v[1] / v[0] for k, v in kt.items()},
             "gpu_launches": launches,
+            "cuda_graph": use_graph,
             "tiles": tiles if tiles else {"chosen": ws.tiles, "autotuned": False},
             "path": "plain" if args.plain else ("batched+learned tail" if tail else "batched"),
             "parity": parity,

@@ -154,6 +154,7 @@ _SIGS = [
                                         C.c_int32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("gx_workspace_create", C.c_int32, [C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(C.c_void_p)]),
     ("gx_workspace_free", C.c_int32, [C.c_void_p]),
+    ("gx_workspace_set_graph", C.c_int32, [C.c_void_p, C.c_int32]),
     ("gx_workspace_get_tiles", C.c_int32, [C.c_void_p, C.POINTER(Tiles)]),
     ("gx_workspace_set_tiles", C.c_int32, [C.c_void_p, C.POINTER(Tiles)]),
     ("gx_autotune", C.c_int32, [C.c_void_p, C.c_void_p, C.POINTER(Queries), C.POINTER(Params), C.c_uint32,

@@ -40,7 +40,13 @@ gx_status fail(gx_status code, const std::string &msg)
     return code;
 }
 
-void count_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+namespace {
+thread_local bool t_capturing = false;   // kernels issued into a graph capture are counted per replay
+}
+void count_launch(uint64_t n)
+{
+    if (!t_capturing) g_launches.fetch_add(n, std::memory_order_relaxed);
+}
 
 // ---- opt-in kernel timing --------------------------------------------------------------
 namespace {
@@ -402,6 +408,16 @@ struct gx_workspace {
     BatchedScratch bs{};
     int tile = kBlockEntries;   // largest candidate tile the buffers hold (the index's block)
     BatchedTiles tiles{};       // launch shape of the batched path (gx_workspace_set_tiles, gx_autotune)
+    // CUDA graphs of the batched launch sequence (gx_workspace_set_graph): one per key of
+    // buffers, parameters, shape and attached tail, the most recent kGraphs kept
+    bool graph_on = false;
+    struct Graph {
+        std::vector<unsigned char> key;
+        cudaGraphExec_t exec = nullptr;
+        uint64_t kernels = 0;
+    };
+    std::vector<Graph> graphs;
+    cudaEvent_t gev_in = nullptr, gev_out = nullptr;
 };
 
 extern "C" const char *gx_last_error(void) { return g_last_error.c_str(); }
@@ -465,6 +481,9 @@ extern "C" gx_status gx_workspace_free(gx_workspace *ws)
                     ws->dMq, ws->out, ws->heap, ws->hist, ws->ivl, ws->nivl, ws->guard, ws->queue,
                     ws->hist_g, ws->spill, ws->logtab, ws->bs.key_in, ws->bs.key_out, ws->bs.ord_in, ws->bs.ord_out, ws->bs.sort_temp};
     for (void *p : ptrs) cudaFree(p);
+    for (auto &g : ws->graphs) cudaGraphExecDestroy(g.exec);
+    if (ws->gev_in) cudaEventDestroy(ws->gev_in);
+    if (ws->gev_out) cudaEventDestroy(ws->gev_out);
     if (ws->stream) cudaStreamDestroy(ws->stream);
     delete ws;
     cudaGetLastError();   // nothing of a free is reported to the next call
@@ -568,7 +587,7 @@ gx_status check_params(const gx_index *ix, const gx_params *p, int32_t *cap)
     return GX_SUCCESS;
 }
 
-gx_status launch_search(gx_index *ix, gx_workspace *ws, const gx_queries *q, const gx_params *p, gx_result *out,
+gx_status launch_direct(gx_index *ix, gx_workspace *ws, const gx_queries *q, const gx_params *p, gx_result *out,
                         gx_cell *heap, uint32_t *hist, cudaStream_t st)
 {
     int32_t cap;
@@ -615,6 +634,96 @@ gx_status launch_search(gx_index *ix, gx_workspace *ws, const gx_queries *q, con
     prof_end(h, st);
     count_launch();
     GX_CUDA(cudaGetLastError());
+    return GX_SUCCESS;
+}
+
+constexpr size_t kGraphs = 4;
+
+// Kernel nodes of a graph (for the launch count of its replays).
+uint64_t kernel_nodes(cudaGraph_t g)
+{
+    size_t n = 0;
+    if (cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess || n == 0) return 0;
+    std::vector<cudaGraphNode_t> nodes(n);
+    if (cudaGraphGetNodes(g, nodes.data(), &n) != cudaSuccess) return 0;
+    uint64_t k = 0;
+    for (auto nd : nodes) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) k++;
+    }
+    return k;
+}
+
+// The batched path's launch sequence through a CUDA graph: captured on the workspace's
+// stream the first time a key (queries, parameters, outputs, launch shape, attached tail)
+// is seen, replayed afterwards; ordered after the caller's earlier work on `st` and before
+// its later work by two events.  The plain path and timed runs (gx_profile_enable) launch
+// directly.
+gx_status launch_search(gx_index *ix, gx_workspace *ws, const gx_queries *q, const gx_params *p, gx_result *out,
+                        gx_cell *heap, uint32_t *hist, cudaStream_t st)
+{
+    if (!ws->graph_on || (p->flags & GX_FLAG_PLAIN) || g_prof_on || q->nspec == 0)
+        return launch_direct(ix, ws, q, p, out, heap, hist, st);
+    int32_t cap;
+    gx_status rc = check_params(ix, p, &cap);   // refused before any capture
+    if (rc != GX_SUCCESS) return rc;
+    if (q->nspec > ws->max_spec || q->npeaks > ws->max_peaks)
+        return fail(GX_ERR_INVLD_SIZE, "more spectra or peaks than the workspace holds");
+    std::vector<unsigned char> key(sizeof(gx_queries) + sizeof(gx_params) + 3 * sizeof(void *) +
+                                   sizeof(BatchedTiles) + sizeof(void *) + sizeof(uint32_t));
+    unsigned char *k = key.data();
+    auto put = [&](const void *v, size_t n) {
+        std::memcpy(k, v, n);
+        k += n;
+    };
+    put(q, sizeof(gx_queries));
+    put(p, sizeof(gx_params));
+    put(&out, sizeof(void *));
+    put(&heap, sizeof(void *));
+    put(&hist, sizeof(void *));
+    put(&ws->tiles, sizeof(BatchedTiles));
+    put(&ws->tail, sizeof(void *));
+    put(&ws->tail_below, sizeof(uint32_t));
+    cudaStream_t gs = ws->stream;
+    gx_workspace::Graph *g = nullptr;
+    for (auto &x : ws->graphs)
+        if (x.key == key) g = &x;
+    if (!g) {
+        cudaGetLastError();
+        GX_CUDA(cudaStreamBeginCapture(gs, cudaStreamCaptureModeThreadLocal));
+        t_capturing = true;
+        rc = launch_direct(ix, ws, q, p, out, heap, hist, gs);
+        t_capturing = false;
+        cudaGraph_t graph = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(gs, &graph);
+        if (rc != GX_SUCCESS || e != cudaSuccess) {
+            if (graph) cudaGraphDestroy(graph);
+            cudaGetLastError();
+            return rc != GX_SUCCESS ? rc : cuda_fail(e, "search graph capture");
+        }
+        gx_workspace::Graph ng;
+        ng.key = std::move(key);
+        ng.kernels = kernel_nodes(graph);
+        const cudaError_t ei = cudaGraphInstantiate(&ng.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ei != cudaSuccess) return cuda_fail(ei, "search graph instantiate");
+        if (ws->graphs.size() >= kGraphs) {
+            cudaGraphExecDestroy(ws->graphs.front().exec);
+            ws->graphs.erase(ws->graphs.begin());
+        }
+        ws->graphs.push_back(std::move(ng));
+        g = &ws->graphs.back();
+    }
+    if (st != gs) {
+        GX_CUDA(cudaEventRecord(ws->gev_in, st));
+        GX_CUDA(cudaStreamWaitEvent(gs, ws->gev_in, 0));
+    }
+    GX_CUDA(cudaGraphLaunch(g->exec, gs));
+    count_launch(g->kernels);
+    if (st != gs) {
+        GX_CUDA(cudaEventRecord(ws->gev_out, gs));
+        GX_CUDA(cudaStreamWaitEvent(st, ws->gev_out, 0));
+    }
     return GX_SUCCESS;
 }
 
@@ -672,6 +781,23 @@ std::mutex g_tune_mu;
 std::map<TuneKey, BatchedTiles> g_tune_cache;
 
 }  // namespace
+
+extern "C" gx_status gx_workspace_set_graph(gx_workspace *ws, int32_t on)
+{
+    if (!ws) return fail(GX_ERR_INVLD_PTR, "gx_workspace_set_graph: null workspace");
+    DeviceScope ds(ws->device);
+    GX_CUDA(ds.status());
+    if (on && !ws->gev_in) {
+        GX_CUDA(cudaEventCreateWithFlags(&ws->gev_in, cudaEventDisableTiming));
+        GX_CUDA(cudaEventCreateWithFlags(&ws->gev_out, cudaEventDisableTiming));
+    }
+    if (!on) {
+        for (auto &g : ws->graphs) cudaGraphExecDestroy(g.exec);
+        ws->graphs.clear();
+    }
+    ws->graph_on = on != 0;
+    return GX_SUCCESS;
+}
 
 extern "C" gx_status gx_workspace_get_tiles(const gx_workspace *ws, gx_tiles *t)
 {

@@ -82,6 +82,11 @@ class Searcher:
         N.check(N.lib().gx_workspace_set_tail(self.handle, model.handle if model else None, sparse_below))
         self._tail = model   # keep the model alive while attached
 
+    def set_graph(self, on: bool = True) -> None:
+        """Capture the batched launch sequence in CUDA graphs and replay them
+        (gx_workspace_set_graph); off releases them."""
+        N.check(N.lib().gx_workspace_set_graph(self.handle, int(on)))
+
     @property
     def tiles(self) -> dict:
         """Launch shape of the batched path (gx_tiles)."""

@@ -262,6 +262,14 @@ typedef struct {
     uint32_t tile;
     uint32_t sorted;
 } gx_tiles;
+/* CUDA graphs for the batched path's launch sequence (on = 1; 0 releases them).  The
+ * sequence (k_prep, sort, k_search_batched, k_tailfit, learned tail) is captured on the
+ * workspace's stream the first time a combination of query and output buffers, parameters,
+ * launch shape and attached tail is seen, and replayed afterwards (the last 4 kept); it is
+ * ordered after the caller's earlier work on its stream, and before its later work, by
+ * events.  The plain path and calls made while gx_profile_enable is on launch directly.
+ * No counterpart in the reference (one launch per kernel per batch). */
+gx_status gx_workspace_set_graph(gx_workspace *ws, int32_t on);
 gx_status gx_workspace_get_tiles(const gx_workspace *ws, gx_tiles *t);
 gx_status gx_workspace_set_tiles(gx_workspace *ws, const gx_tiles *t);
 #define GX_TUNE_MAX 32

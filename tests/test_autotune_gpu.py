@@ -82,3 +82,38 @@ def test_invalid_shapes_are_refused(setup):
     with pytest.raises(gx.GxError) as e:
         s.autotune(qd, gx.SearchParams(dM=MULTIBLOCK["dM"], flags=gx.FLAG_PLAIN))
     assert e.value.code == -3002
+
+
+def test_graph_replay_equals_direct_launches(setup):
+    """The launch sequence captured in a CUDA graph and replayed gives the same records as
+    direct launches: on the first (capturing) call, on a replay, after a change of
+    parameters (a new capture), through the device entry point on the caller's stream and
+    through the host entry point; each replay counts its kernels."""
+    gx, torch, s, q, p, qd, keep = setup
+    import dataclasses
+    import gicops_b200._native as N
+    ref = s.search(q, p, heap=True, hist=True)
+    p2 = dataclasses.replace(p, topmatches=10, min_shp=5)
+    ref2 = s.search(q, p2).result
+    d = torch.device("cuda", 0)
+    out = torch.empty(q.n * N.RESULT_DTYPE.itemsize, dtype=torch.uint8, device=d)
+    stream = torch.cuda.current_stream().cuda_stream
+    s.search_device(qd, p, out.data_ptr(), stream=stream)
+    torch.cuda.synchronize()
+    direct_dev = out.cpu().numpy().copy()
+    s.set_graph(True)
+    try:
+        for _ in range(2):
+            r = s.search(q, p, heap=True, hist=True)
+            assert r.result.tobytes() == ref.result.tobytes() and r.heap.tobytes() == ref.heap.tobytes()
+            assert np.array_equal(r.hist, ref.hist)
+        assert s.search(q, p2).result.tobytes() == ref2.tobytes()
+        for _ in range(2):
+            out.zero_()
+            n0 = gx.lib().gx_launch_count()
+            s.search_device(qd, p, out.data_ptr(), stream=stream)
+            torch.cuda.synchronize()
+            assert gx.lib().gx_launch_count() - n0 >= 4
+            assert out.cpu().numpy().tobytes() == direct_dev.tobytes()
+    finally:
+        s.set_graph(False)
