@@ -469,19 +469,29 @@ def parity_block(gx, N, H, q, params, w, run_full, tail_on: bool, n_sample: int 
     e_rel = rel(res["e_x"][plain & fin], o["e_x"][plain & fin])
     fp64_rel = rel(res["e_fp64"][fin], o["e_fp64"][fin])
     slope_rel = rel(res["slope"][fin], o["slope"][fin])
-    # hyperscore of the top PSM in FP32 against its FP64 value (oracle scorecard of the spectrum)
+    # hyperscore of the top PSM in FP32 against its FP64 value, from that candidate's matched
+    # ions counted in the index's own buckets (dslim_query.cpp:853-914 for one candidate)
     lg = pyoracle.lgfact()
     hyp_err = 0.0
+    dF = params.dF
     for i in np.nonzero(fitted)[0][:n_hyp]:
-        a0, a1 = int(sq.idx[i]), int(sq.idx[i + 1])
-        dm = w["dM"] if sq.dM is None or np.isnan(sq.dM[i]) else float(sq.dM[i])
-        c = pyoracle.candidates(H.lengths, sq.moz[a0:a1], sq.intn[a0:a1], float(sq.prec[i]), dm,
-                                pyoracle.Params(dM=dm), cap=1 << 23)
         t = res["top"][i]
-        m = c[(c["ixx"] == t["idxoffset"]) & (c["psid"] == t["psid"])]
-        if len(m):
-            bc, yc = min(int(m["bc"][0]), 80), min(int(m["yc"][0]), 80)
-            h64 = lg[bc] + lg[yc] + np.log10(1.0 + float(m["ibc"][0])) + np.log10(1.0 + float(m["iyc"][0])) - 4.0
+        ln = H.lengths[int(t["idxoffset"])]
+        speclen = int(ln["speclen"])
+        bA, iA = ln["bA"], ln["iA"]
+        a0, a1 = int(sq.idx[i]), int(sq.idx[i + 1])
+        bc = yc = ibc = iyc = 0
+        for mz, it in zip(sq.moz[a0:a1].astype(np.int64), sq.intn[a0:a1].astype(np.int64)):
+            if not (mz > dF and mz < params.max_mass * params.scale - 1 - dF):
+                continue
+            ids = iA[int(bA[mz - dF]):int(bA[mz + dF + 1])].astype(np.int64)
+            hit = ids[ids // speclen == int(t["psid"])]
+            ny = int(np.count_nonzero((hit % speclen) // (speclen // 2)))
+            nb = len(hit) - ny
+            bc, yc, ibc, iyc = bc + nb, yc + ny, ibc + nb * int(it), iyc + ny * int(it)
+        ibc, iyc = ibc % (1 << 32), iyc % (1 << 32)
+        h64 = lg[min(bc, 80)] + lg[min(yc, 80)] + np.log10(1.0 + ibc) + np.log10(1.0 + iyc) - 4.0
+        if bc + yc == int(t["sharedions"]) and 0 < h64 < 80:   # hyperscores of 80 and above are clamped to 79
             hyp_err = max(hyp_err, abs(float(t["hyperscore"]) - h64) / abs(h64))
     # the reference's e-value (slope/intercept truncated to 1e-6) against the unquantized fit
     q_fit = plain & fin & (res["e_x"] > 0)

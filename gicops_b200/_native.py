@@ -107,7 +107,7 @@ class StreamStats(C.Structure):
 
 class Tiles(C.Structure):
     _fields_ = [("chunks_per_lane", C.c_uint32), ("ctas_per_sm", C.c_uint32), ("tile", C.c_uint32),
-                ("sorted", C.c_uint32)]
+                ("sorted", C.c_uint32), ("pipeline", C.c_uint32)]
 
     def as_dict(self) -> dict:
         return {f: int(getattr(self, f)) for f, _ in self._fields_}

@@ -304,7 +304,8 @@ __device__ __forceinline__ void scatter_wide(uint32_t *cnt, uint32_t *ib, uint32
 // histogram and candidate count take every PSM; PSMs with h >= tau go, in order, to the
 // warp's entrant list for the exact heap.  Per 64 candidates, all scorecard reads and
 // log10 table loads are issued before any hyperscore is formed.
-__device__ __forceinline__ void score_batch(BatchSmem &sm, const BatchDyn &dd, const SearchArgs &a, const void *scv,
+template <class SM, int ENT_SMEM>
+__device__ __forceinline__ void score_batch(SM &sm, const uint32_t *pend, const SearchArgs &a, const void *scv,
                                             int ctile, int wid, int lane, int n, int t0, int ixx, uint32_t speclen,
                                             float tau, bool wide, Cell *ent, int &nent, int &cps)
 {
@@ -316,7 +317,7 @@ __device__ __forceinline__ void score_batch(BatchSmem &sm, const BatchDyn &dd, c
     for (int g = 0; g < kG; g++) {
         off[g] = 0; bc[g] = yc[g] = ib[g] = iy[g] = 0;
         if (q0 + 32 * g + lane < n) {
-            off[g] = dd.pend[wid][q0 + 32 * g + lane];
+            off[g] = pend[q0 + 32 * g + lane];
             if (!wide) {
                 const uint2 v = reinterpret_cast<const uint2 *>(scv)[off[g]];
                 bc[g] = v.x >> 24; ib[g] = v.x & 0xFFFFFFu; yc[g] = v.y >> 24; iy[g] = v.y & 0xFFFFFFu;
@@ -373,8 +374,12 @@ __device__ __forceinline__ void score_batch(BatchSmem &sm, const BatchDyn &dd, c
         const unsigned eb = __ballot_sync(0xffffffffu, e);
         if (e) {
             const int gi = nent + __popc(eb & ((1u << lane) - 1u));
-            if (gi < kEntSmem) sm.ent_s[wid][gi] = cell;
-            else ent[gi] = cell;
+            if constexpr (ENT_SMEM > 0) {
+                if (gi < ENT_SMEM) sm.ent_s[wid][gi] = cell;
+                else ent[gi] = cell;
+            } else {
+                ent[gi] = cell;
+            }
         }
         nent += __popc(eb);
     }
@@ -638,6 +643,13 @@ __device__ __forceinline__ void stream_tile(BatchSmem &sm, const BatchDyn &dd, c
     }
 }
 
+// Whether k_search_piped takes spectrum s (k_search_batched takes the others).
+__device__ __forceinline__ bool piped_spectrum(const SearchArgs &a, uint32_t s)
+{
+    const uint32_t nv = a.nivl[s];
+    return a.guard[s] == 1u && nv >= 1u && nv <= (uint32_t)kIvlChunk && !(a.flags & GX_FLAG_WIDE_SCORECARD);
+}
+
 template <int CH>
 __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchArgs a)
 {
@@ -667,8 +679,17 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
     for (;;) {
         __syncthreads();
         if (tid == 0) {
-            const uint32_t slot = atomicAdd(a.queue, 1u);
-            sm.spec = slot < a.nspec ? (int32_t)a.order[slot] : -1;
+            int32_t spec = -1;
+            for (;;) {   // with a.split, the spectra k_search_piped takes are left to it
+                const uint32_t slot = atomicAdd(a.queue, 1u);
+                if (slot >= a.nspec) break;
+                const uint32_t s2 = a.order[slot];
+                if (!a.split || !piped_spectrum(a, s2)) {
+                    spec = (int32_t)s2;
+                    break;
+                }
+            }
+            sm.spec = spec;
             sm.heap_size = 0;
             sm.cpsms = 0;
             sm.status = 0;
@@ -823,7 +844,8 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
                         if (total == 0) continue;
                         if (npend + total > kPend) {   // queue full: score what it holds first
                             __syncwarp();
-                            score_batch(sm, dd, a, scv, ctile, wid, lane, npend, t0, ixx, speclen, tau, wide, ent, nent, cps);
+                            score_batch<BatchSmem, kEntSmem>(sm, dd.pend[wid], a, scv, ctile, wid, lane, npend, t0, ixx, speclen, tau, wide, ent,
+                                                      nent, cps);
                             __syncwarp();
                             clear_scored(sw, dd.pend[wid], npend, lane);
                             npend = 0;
@@ -874,7 +896,8 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
                     if (total == 0) continue;
                     if (npend + total > kPend) {   // queue full: score what it holds first
                         __syncwarp();
-                        score_batch(sm, dd, a, scv, ctile, wid, lane, npend, t0, ixx, speclen, tau, wide, ent, nent, cps);
+                        score_batch<BatchSmem, kEntSmem>(sm, dd.pend[wid], a, scv, ctile, wid, lane, npend, t0, ixx, speclen, tau, wide, ent,
+                                                      nent, cps);
                         __syncwarp();
                         if (!wide && GX_FUSED_CLEAR) clear_scored(sw, dd.pend[wid], npend, lane);
                         npend = 0;
@@ -886,7 +909,8 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
                 }
                 __syncwarp();
                 if (npend > 0) {
-                    score_batch(sm, dd, a, scv, ctile, wid, lane, npend, t0, ixx, speclen, tau, wide, ent, nent, cps);
+                    score_batch<BatchSmem, kEntSmem>(sm, dd.pend[wid], a, scv, ctile, wid, lane, npend, t0, ixx, speclen, tau, wide, ent,
+                                                      nent, cps);
                     __syncwarp();
                     if (!wide && GX_FUSED_CLEAR) clear_scored(sw, dd.pend[wid], npend, lane);
                 }
@@ -963,6 +987,449 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
 
 
 // ------------------------------------------------------------------------------------
+// k_search_piped: one CTA of 32 warps per SM with two scorecard tiles.  In phase p every
+// warp scans and scores its range of tile p - 1 (one buffer), then takes work units of
+// tile p's ids (the other buffer) until none are left; warp 0 prepares tile p + 1 (its
+// descriptor and span table) and the last warp first inserts tile p - 2's heap entrants.
+// One barrier per tile, and the stream's dynamic units absorb the uneven scoring.  It
+// takes the spectra with the 8-byte scorecard and at most kIvlChunk intervals (almost all
+// of them); k_search_batched takes the rest in a second launch.
+// ------------------------------------------------------------------------------------
+constexpr int kPWarps = 32;
+constexpr int kPBlock = kPWarps * 32;
+constexpr int kPPend = 136;                  // per-warp queue: one scan step (128) + slack
+constexpr int kPHeapWarp = kPWarps - 1;
+static_assert(kPPend >= 128, "the queue must hold one scan step's candidates (32 lanes x 4)");
+
+struct PipedTile {
+    int32_t valid;
+    int32_t ixx;
+    int32_t t0, tn;
+    uint32_t lo, lim;       // block-local id range of the tile: id - lo < lim
+    int32_t whole;          // the tile is its whole block
+    uint32_t speclen;
+    uint64_t base;          // 16-byte aligned element offset of the length's ids in iAb
+};
+
+struct PipedSmem {
+    uint32_t hist[kHist];
+    double lgf[81];
+    Cell heap[kMaxHeap + 1];
+    int32_t warp_cnt[2][kPWarps];   // entrants per warp, by tile parity
+    uint32_t ent_mask[2];
+    uint32_t next_unit[2];          // work-unit counter of the tile streaming into buffer b
+    int32_t heap_size;
+    int32_t cpsms;
+    int32_t status;
+    int32_t spec;
+    float tau;                      // entrant threshold: -1 while the heap is not full, then its root
+    int32_t it_ixx;                 // tile iterator (written by warp 0)
+    int64_t it_kb, it_kb1;
+    uint4 keep_lo[8];
+    uint4 keep_hi[8];
+    PipedTile tile[3];              // tiles p - 1 (scanned), p (streamed), p + 1 (prepared): by tile number mod 3
+};
+
+struct PipedDyn {
+    uint32_t *card[2];              // scorecard words [2T] + kDummy dummy words, per buffer
+    uint32_t (*pend)[kPPend];
+    uint4 *sp_rec[2];
+    uint32_t *sp_pre[2];
+};
+
+__host__ __device__ constexpr size_t piped_card_words(int tile) { return 2 * (size_t)tile + kDummy; }
+
+__host__ __device__ constexpr size_t piped_dyn_bytes(int tile)
+{
+    return sizeof(uint32_t) * (2 * piped_card_words(tile) + (size_t)kPWarps * kPPend +
+                               2 * (4 * (size_t)kIvlChunk + (kIvlChunk + 4)));
+}
+
+__device__ __forceinline__ PipedDyn carve_piped(unsigned char *base, int tile)
+{
+    PipedDyn d;
+    uint32_t *p = reinterpret_cast<uint32_t *>(base);
+    d.card[0] = p; p += piped_card_words(tile);
+    d.card[1] = p; p += piped_card_words(tile);
+    d.pend = reinterpret_cast<uint32_t (*)[kPPend]>(p); p += (size_t)kPWarps * kPPend;
+    for (int b = 0; b < 2; b++) {   // 16-byte aligned: every block above is a multiple of 4 words
+        d.sp_rec[b] = reinterpret_cast<uint4 *>(p); p += 4 * kIvlChunk;
+        d.sp_pre[b] = p; p += kIvlChunk + 4;
+    }
+    return d;
+}
+
+// Warp 0: the next tile of spectrum s (the next entry block of the current length's window,
+// or the first block of the next length with a window) into slot `slot`, with its span table
+// in buffer b: per interval, its chunk offset, id range and add value, and the exclusive
+// prefix of the intervals' 16-byte chunk counts.  Resets buffer b's unit counter.
+__device__ void piped_prepare(PipedSmem &sm, const PipedDyn &dd, const SearchArgs &a, int s, const Interval *ivl,
+                              uint32_t nv, int slot, int b, int lane)
+{
+    int ixx = sm.it_ixx;
+    int64_t kb = sm.it_kb + 1, kb1 = sm.it_kb1;
+    const int64_t E = a.block;
+    if (kb > kb1) {
+        for (ixx = ixx + 1; ixx < a.nlen; ixx++) {
+            const int2 w = a.win[(uint64_t)s * a.nlen + ixx];
+            if (w.y >= w.x) {
+                kb = w.x / E;
+                kb1 = w.y / E;
+                break;
+            }
+        }
+    }
+    __syncwarp();
+    if (ixx >= a.nlen) {
+        if (lane == 0) {
+            sm.tile[slot].valid = 0;
+            sm.it_ixx = ixx;
+        }
+        return;
+    }
+    const int2 w = a.win[(uint64_t)s * a.nlen + ixx];
+    const DevLen ln = a.lens[ixx];
+    const int t0 = (int)max((int64_t)w.x, kb * E), t1 = (int)min((int64_t)w.y + 1, (kb + 1) * E);
+    const uint64_t base = ln.ia_off & ~7ull;
+    const uint32_t rel0 = (uint32_t)(ln.ia_off - base);
+    const uint32_t *__restrict__ bA = a.blkA + ln.blk_off + (uint64_t)kb * (a.nbins + 1);
+    constexpr int kPer = kIvlChunk / 32;
+    uint32_t cnt[kPer], q0s[kPer];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int j = 0; j < kPer; j++) {
+        const uint32_t i = (uint32_t)lane * kPer + j;
+        cnt[j] = 0;
+        q0s[j] = 0;
+        if (i < nv) {
+            const Interval v = ivl[i];
+            const uint32_t a0 = rel0 + __ldg(bA + v.b0), a1 = rel0 + __ldg(bA + v.b1 + 1);
+            const uint32_t q0 = a0 >> 3;
+            cnt[j] = a1 > a0 ? ((a1 + 7u) >> 3) - q0 : 0u;
+            q0s[j] = q0;
+            dd.sp_rec[b][i] = make_uint4(0u, a0, a1, (v.c << 24) | v.S);
+            sum += cnt[j];
+        }
+    }
+    uint32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    uint32_t run = incl - sum;
+#pragma unroll
+    for (int j = 0; j < kPer; j++) {
+        const uint32_t i = (uint32_t)lane * kPer + j;
+        if (i < nv) {
+            dd.sp_pre[b][i] = run;
+            dd.sp_rec[b][i].x = q0s[j] - run;
+        }
+        run += cnt[j];
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    if (lane == 0) {
+        dd.sp_pre[b][nv] = total;
+        sm.next_unit[b] = 0;
+        PipedTile t;
+        t.valid = 1;
+        t.ixx = ixx;
+        t.t0 = t0;
+        t.tn = t1 - t0;
+        t.lo = 2u * (uint32_t)(t0 - kb * E);
+        t.lim = 2u * (uint32_t)(t1 - t0);
+        t.whole = ((int64_t)t0 == kb * E && (int64_t)t1 == min((kb + 1) * E, (int64_t)ln.npep)) ? 1 : 0;
+        t.speclen = ln.speclen;
+        t.base = base;
+        sm.tile[slot] = t;
+        sm.it_ixx = ixx;
+        sm.it_kb = kb;
+        sm.it_kb1 = kb1;
+    }
+}
+
+// The ids of every interval of a span table into an 8-byte scorecard (stream_tile's packed
+// path: units of 32 x CH 16-byte chunks from a shared counter, keep masks for the ids of
+// an interval's first and last chunk that lie outside it, the lane's dummy word for ids
+// outside the tile).
+template <int CH>
+__device__ __forceinline__ void piped_stream(uint32_t *next_unit, const uint4 *keep_lo, const uint4 *keep_hi,
+                                             const uint4 *sp_rec, const uint32_t *sp_pre,
+                                             const uint4 *__restrict__ ia4, uint32_t ncv, uint32_t *cnt, int ctile,
+                                             bool whole, uint32_t lo, uint32_t lim, int lane)
+{
+    const uint32_t M = sp_pre[ncv];
+    const uint32_t dummy = 2u * (uint32_t)ctile + (uint32_t)lane;
+    const uint32_t fill = whole ? (dummy | (dummy << 16)) : 0xFFFFFFFFu;
+    for (;;) {
+        uint32_t u = 0;
+        if (lane == 0) u = atomicAdd(next_unit, 1u);
+        u = __shfl_sync(0xffffffffu, u, 0);
+        const uint32_t j0 = u * (32u * CH);
+        if (j0 >= M) break;
+        const uint32_t s1 = (uint32_t)lane * 8u;
+        const uint32_t b1 = __ballot_sync(0xffffffffu, s1 < ncv && sp_pre[s1] <= j0);
+        const uint32_t base = (31u - (uint32_t)__clz(b1)) * 8u;
+        const uint32_t s2 = base + ((uint32_t)lane & 7u);
+        const uint32_t b2 = __ballot_sync(0xffffffffu, lane < 8 && s2 < ncv && sp_pre[s2] <= j0);
+        uint32_t k = base + (31u - (uint32_t)__clz(b2));
+        uint4 v[CH];
+        uint32_t kx[CH];
+#pragma unroll
+        for (int p = 0; p < CH; p++) {
+            const uint32_t j = j0 + (uint32_t)lane + 32u * p;
+            kx[p] = 0xFFFFFFFFu;
+            if (j < M) {
+                while (sp_pre[k + 1] <= j) k++;
+                kx[p] = k;
+                v[p] = __ldg(ia4 + (sp_rec[k].x + j));
+            }
+        }
+#pragma unroll
+        for (int p = 0; p < CH; p++) {
+            if (kx[p] == 0xFFFFFFFFu) continue;
+            const uint4 r = sp_rec[kx[p]];
+            const uint32_t j = j0 + (uint32_t)lane + 32u * p;
+            const uint32_t eq = (r.x + j) << 3;
+            const uint32_t mlo = r.y > eq ? r.y - eq : 0u;
+            const uint32_t mhi = min(r.z - eq, 8u);
+            const uint4 kl = keep_lo[mlo], kh = keep_hi[mhi - 1u];
+            uint32_t w4[4] = {v[p].x, v[p].y, v[p].z, v[p].w};
+            const uint32_t km[4] = {kl.x & kh.x, kl.y & kh.y, kl.z & kh.z, kl.w & kh.w};
+#pragma unroll
+            for (int q = 0; q < 4; q++) w4[q] = (w4[q] & km[q]) | (fill & ~km[q]);
+            if (whole) {
+#pragma unroll
+                for (int m = 0; m < 8; m++) atomicAdd(cnt + ((w4[m >> 1] >> (16 * (m & 1))) & 0xFFFFu), r.w);
+            } else {
+#pragma unroll
+                for (int m = 0; m < 8; m++)
+                    scatter_packed(cnt, (w4[m >> 1] >> (16 * (m & 1))) & 0xFFFFu, lo, lim, r.w, dummy, true);
+            }
+        }
+    }
+}
+
+// Warp kPHeapWarp: the entrants of the tile of parity `par` into the heap, in warp order
+// (each warp's list is in candidate order), as insert_entrants does (lists in global memory).
+__device__ __noinline__ void piped_insert(PipedSmem &sm, const Cell *lists, uint32_t stride, int par, int cap,
+                                          int lane)
+{
+    int hs = sm.heap_size;
+    for (uint32_t mask = sm.ent_mask[par]; mask; mask &= mask - 1u) {
+        const int w2 = __ffs(mask) - 1;
+        const int n2 = sm.warp_cnt[par][w2];
+        const Cell *e2 = lists + ((uint64_t)par * kPWarps + w2) * stride;
+        Cell nxt;
+        if (lane < n2) nxt = e2[lane];
+        for (int k0 = 0; k0 < n2; k0 += 32) {
+            const Cell c = nxt;
+            const bool v = k0 + lane < n2;
+            const int k1 = k0 + 32 + lane;
+            if (k1 < n2) nxt = e2[k1];
+            __syncwarp();
+            const float root = hs == cap ? sm.heap[0].h : -INFINITY;
+            uint32_t live = __ballot_sync(0xffffffffu, v && c.h >= root);
+            const uint32_t u1 = ((uint32_t)c.ixx) | ((uint32_t)c.shp << 16);
+            const uint32_t u2 = ((uint32_t)c.total) | ((uint32_t)c.pad << 16);
+            while (live) {
+                const int j = __ffs(live) - 1;
+                live &= live - 1u;
+                Cell cj;
+                cj.h = __shfl_sync(0xffffffffu, c.h, j);
+                cj.psid = __shfl_sync(0xffffffffu, c.psid, j);
+                const uint32_t v1 = __shfl_sync(0xffffffffu, u1, j), v2 = __shfl_sync(0xffffffffu, u2, j);
+                cj.ixx = (uint16_t)(v1 & 0xFFFFu); cj.shp = (uint16_t)(v1 >> 16);
+                cj.total = (uint16_t)(v2 & 0xFFFFu); cj.pad = (uint16_t)(v2 >> 16);
+                if (lane == 0) {
+                    int h0 = hs;
+                    heap_insert(sm.heap, h0, cap, cj);
+                }
+                hs = min(hs + 1, cap);
+            }
+        }
+    }
+    __syncwarp();
+    if (lane == 0) {
+        sm.heap_size = hs;
+        sm.ent_mask[par] = 0u;
+        *reinterpret_cast<volatile float *>(&sm.tau) = hs == cap ? sm.heap[0].h : -1.0f;
+    }
+}
+
+template <int CH>
+__global__ void __launch_bounds__(kPBlock, 1) k_search_piped(SearchArgs a)
+{
+    extern __shared__ __align__(16) unsigned char dyn[];
+    __shared__ PipedSmem sm;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    for (int i = tid; i < 81; i += kPBlock) sm.lgf[i] = a.lgfact[i];
+    if (tid < 16) {   // keep masks (table lo: ids >= m; table hi: ids < m + 1)
+        const int m = tid & 7;
+        uint32_t w[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const bool k0 = tid < 8 ? 2 * q >= m : 2 * q < m + 1;
+            const bool k1 = tid < 8 ? 2 * q + 1 >= m : 2 * q + 1 < m + 1;
+            w[q] = (k0 ? 0x0000FFFFu : 0u) | (k1 ? 0xFFFF0000u : 0u);
+        }
+        (tid < 8 ? sm.keep_lo : sm.keep_hi)[m] = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+    const int T = a.tile;   // the index's block: every tile is (part of) one block
+    const PipedDyn dd = carve_piped(dyn, T);
+    for (size_t i = tid; i < 2 * piped_card_words(T); i += kPBlock) dd.card[0][i] = 0u;
+    // entrant lists of this CTA: [parity][warp][stride]
+    const uint32_t stride = a.spill_per_warp / 2u;
+    const Cell *lists = a.spill + (uint64_t)blockIdx.x * 2 * kPWarps * stride;
+    const uint32_t minshp = a.min_shp;
+
+    for (;;) {
+        __syncthreads();
+        if (tid == 0) {
+            int spec = -1;
+            for (;;) {
+                const uint32_t slot = atomicAdd(a.queue, 1u);
+                if (slot >= a.nspec) break;
+                const uint32_t s = a.order[slot];
+                if (piped_spectrum(a, s)) {
+                    spec = (int)s;
+                    break;
+                }
+            }
+            sm.spec = spec;
+            sm.heap_size = 0;
+            sm.cpsms = 0;
+            sm.status = 0;
+            sm.tau = -1.0f;
+            sm.ent_mask[0] = sm.ent_mask[1] = 0u;
+            sm.it_ixx = -1;
+            sm.it_kb = 0;
+            sm.it_kb1 = -1;
+        }
+        for (int i = tid; i < kHist; i += kPBlock) sm.hist[i] = 0;
+        __syncthreads();
+        const int s = sm.spec;
+        if (s < 0) break;
+        const uint32_t nv = a.nivl[s];
+        const Interval *ivl = a.ivl + 2ull * a.qidx[s];
+        if (wid == 0) piped_prepare(sm, dd, a, s, ivl, nv, 0, 0, lane);
+        __syncthreads();
+        int cps = 0;
+        int last_par = -1;   // parity of the last scanned tile (its entrants wait for the end)
+        for (int p = 0;; p++) {
+            const int bs = (p + 1) & 1, bt = p & 1;   // buffers of tiles p - 1 and p
+            const PipedTile ts = sm.tile[(p + 2) % 3], tt = sm.tile[p % 3];
+            const bool scan = p > 0 && ts.valid;
+            const bool strm = tt.valid != 0;
+            if (!scan && !strm) break;
+            if (wid == kPHeapWarp && p >= 2) piped_insert(sm, lists, stride, bt, a.heap_cap, lane);
+            if (scan) {
+                // ---- scan and score tile p - 1: warp w owns [w R, (w + 1) R), four candidates per lane per step
+                const float tau = *reinterpret_cast<volatile float *>(&sm.tau);
+                const int tn = ts.tn;
+                const int R = ((tn + kPWarps - 1) / kPWarps + 127) / 128 * 128;
+                const int r0 = min(tn, wid * R), r1 = min(tn, r0 + R);
+                uint32_t *sw = dd.card[bs];
+                uint32_t *pend = dd.pend[wid];
+                Cell *ent = const_cast<Cell *>(lists) + ((uint64_t)bs * kPWarps + wid) * stride;
+                int npend = 0, nent = 0;
+                for (int c0 = r0; c0 < r1; c0 += 128) {
+                    unsigned m = 0;
+                    const int cb = c0 + 4 * lane;
+                    if (cb < r1) {
+                        uint4 *z = reinterpret_cast<uint4 *>(sw + 2 * cb);
+                        const uint4 qa = z[0], qb = z[1];
+                        const int lim4 = r1 - cb;
+                        m = ((((qa.x >> 24) + (qa.y >> 24)) >= minshp) ? 1u : 0u) |
+                            ((((qa.z >> 24) + (qa.w >> 24)) >= minshp && lim4 > 1) ? 2u : 0u) |
+                            ((((qb.x >> 24) + (qb.y >> 24)) >= minshp && lim4 > 2) ? 4u : 0u) |
+                            ((((qb.z >> 24) + (qb.w >> 24)) >= minshp && lim4 > 3) ? 8u : 0u);
+                        if (m == 0u) {   // no PSM among the four: reset them for the tile after next
+                            z[0] = make_uint4(0u, 0u, 0u, 0u);
+                            z[1] = make_uint4(0u, 0u, 0u, 0u);
+                        }
+                    }
+                    const unsigned lt = (1u << lane) - 1u;
+                    const unsigned B0 = __ballot_sync(0xffffffffu, m & 1u), B1 = __ballot_sync(0xffffffffu, m & 2u);
+                    const unsigned B2 = __ballot_sync(0xffffffffu, m & 4u), B3 = __ballot_sync(0xffffffffu, m & 8u);
+                    const int total = __popc(B0) + __popc(B1) + __popc(B2) + __popc(B3);
+                    if (total == 0) continue;
+                    if (npend + total > kPPend) {
+                        __syncwarp();
+                        score_batch<PipedSmem, 0>(sm, pend, a, sw, T, wid, lane, npend, ts.t0, ts.ixx, ts.speclen, tau,
+                                                  false, ent, nent, cps);
+                        __syncwarp();
+                        for (int i = lane; i < npend; i += 32) {
+                            uint4 *z = reinterpret_cast<uint4 *>(sw + 2 * (pend[i] & ~3u));
+                            z[0] = make_uint4(0u, 0u, 0u, 0u);
+                            z[1] = make_uint4(0u, 0u, 0u, 0u);
+                        }
+                        npend = 0;
+                        __syncwarp();
+                    }
+                    int pos = npend + __popc(B0 & lt) + __popc(B1 & lt) + __popc(B2 & lt) + __popc(B3 & lt);
+                    for (unsigned mm = m; mm; mm &= mm - 1u) pend[pos++] = (uint32_t)(cb + __ffs(mm) - 1);
+                    npend += total;
+                }
+                __syncwarp();
+                if (npend > 0) {
+                    score_batch<PipedSmem, 0>(sm, pend, a, sw, T, wid, lane, npend, ts.t0, ts.ixx, ts.speclen, tau,
+                                              false, ent, nent, cps);
+                    __syncwarp();
+                    for (int i = lane; i < npend; i += 32) {
+                        uint4 *z = reinterpret_cast<uint4 *>(sw + 2 * (pend[i] & ~3u));
+                        z[0] = make_uint4(0u, 0u, 0u, 0u);
+                        z[1] = make_uint4(0u, 0u, 0u, 0u);
+                    }
+                }
+                if (lane == 0) {
+                    sm.warp_cnt[bs][wid] = nent;
+                    if (nent) atomicOr(&sm.ent_mask[bs], 1u << wid);
+                }
+                last_par = bs;
+            }
+            // ---- warp 0 prepares tile p + 1 (slot (p + 1) mod 3, buffer bs: tile p - 1's)
+            if (wid == 0) piped_prepare(sm, dd, a, s, ivl, nv, (p + 1) % 3, bs, lane);
+            // ---- stream tile p into buffer bt
+            if (strm) {
+                const uint4 *__restrict__ ia4 = reinterpret_cast<const uint4 *>(a.iAb + tt.base);
+                piped_stream<CH>(&sm.next_unit[bt], sm.keep_lo, sm.keep_hi, dd.sp_rec[bt], dd.sp_pre[bt], ia4, nv,
+                                 dd.card[bt], T, tt.whole != 0, tt.lo, tt.lim, lane);
+            }
+            __syncthreads();
+        }
+        if (last_par >= 0 && wid == kPHeapWarp) piped_insert(sm, lists, stride, last_par, a.heap_cap, lane);
+        if (lane == 0 && cps) atomicAdd(&sm.cpsms, cps);
+        __syncthreads();
+        // ---- per-spectrum outputs (the tail fit runs in k_tailfit)
+        for (int i = tid; i < kHist; i += kPBlock) a.hist_g[(uint64_t)s * kHist + i] = sm.hist[i];
+        if (a.heap_out)
+            for (int i = tid; i < a.heap_cap; i += kPBlock) {
+                gx_cell o{};
+                if (i < sm.heap_size) {
+                    const Cell c = sm.heap[i];
+                    o.hyperscore = c.h; o.psid = c.psid; o.idxoffset = c.ixx; o.sharedions = c.shp;
+                    o.totalions = c.total;
+                }
+                a.heap_out[(uint64_t)s * a.heap_cap + i] = o;
+            }
+        if (tid == 0) {
+            gx_result r;
+            memset(&r, 0, sizeof(r));
+            r.cpsms = sm.cpsms;
+            r.status = sm.status;
+            if (fits_tail(sm.cpsms, a.min_cpsm)) {
+                const Cell t = heap_getmax(sm.heap, sm.heap_size);
+                r.top.hyperscore = t.h; r.top.psid = t.psid; r.top.idxoffset = t.ixx;
+                r.top.sharedions = t.shp; r.top.totalions = t.total;
+                r.maxhyp = __double2int_rz(__dadd_rn((double)__fmul_rn(t.h, 10.0f), 0.5));
+            }
+            a.out[s] = r;
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------
 // k_tailfit: one warp per spectrum (the FP64 fit itself is serial in lane 0)
 // ------------------------------------------------------------------------------------
 constexpr int kTfWarps = 4;
@@ -1022,7 +1489,32 @@ SearchKernel search_kernel(int chunks)
     default: return k_search_batched<2>;
     }
 }
+SearchKernel piped_kernel(int chunks)
+{
+    switch (chunks) {
+    case 1: return k_search_piped<1>;
+    case 3: return k_search_piped<3>;
+    default: return k_search_piped<2>;
+    }
+}
 }  // namespace
+
+// Whether one CTA of k_search_piped<chunks> fits an SM at this tile size.
+bool piped_fits(int tile, int chunks)
+{
+    int n = 0;
+    if (cudaFuncSetAttribute(piped_kernel(chunks), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)piped_dyn_bytes(tile)) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, piped_kernel(chunks), kPBlock, piped_dyn_bytes(tile)) !=
+        cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return n >= 1;
+}
 
 // CTAs of k_search_batched<chunks> that fit one SM at this tile size (at most kCtasPerSm).
 int batched_ctas_per_sm(int tile, int chunks)
@@ -1053,7 +1545,8 @@ cudaError_t batched_set_attributes(int tile)
 bool batched_tiles_valid(const BatchedTiles &t, int max_tile)
 {
     return t.chunks >= 1 && t.chunks <= kMaxChunks && t.ctas_per_sm >= 1 && t.ctas_per_sm <= kCtasPerSm &&
-           t.tile >= kMinTile && t.tile <= max_tile && t.tile % 32 == 0 && (t.sorted == 0 || t.sorted == 1);
+           t.tile >= kMinTile && t.tile <= max_tile && t.tile % 32 == 0 && (t.sorted == 0 || t.sorted == 1) &&
+           (t.pipeline == 0 || (t.pipeline == 1 && t.tile == max_tile));
 }
 
 cudaError_t launch_batched(SearchArgs a, const BatchedScratch &b, const BatchedTiles &t, cudaStream_t st)
@@ -1076,7 +1569,17 @@ cudaError_t launch_batched(SearchArgs a, const BatchedScratch &b, const BatchedT
         if (e != cudaSuccess) return e;
         a.order = b.ord_out;
     }
-    if ((e = cudaMemsetAsync(a.queue, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(a.queue, 0, 2 * sizeof(uint32_t), st)) != cudaSuccess) return e;
+    if (t.pipeline) {   // the pipelined kernel first, on its own queue counter; the batched one takes the rest
+        SearchArgs ap = a;
+        ap.queue = a.queue + 1;
+        h = prof_begin("k_search_piped", st);
+        piped_kernel(t.chunks)<<<b.sms, kPBlock, piped_dyn_bytes(a.tile), st>>>(ap);
+        prof_end(h, st);
+        count_launch();
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        a.split = 1;
+    }
     const int ctas = t.ctas_per_sm < b.max_ctas[t.chunks] ? t.ctas_per_sm : b.max_ctas[t.chunks];
     h = prof_begin("k_search_batched", st);
     search_kernel(t.chunks)<<<b.sms * ctas, kBBlock, batched_dyn_smem(a.tile), st>>>(a);

@@ -93,7 +93,8 @@ struct SearchArgs {
     uint32_t *guard;      // [nspec]: 1 if the packed scorecard is exact for the spectrum, 0 if not,
                           // 2 if the spectrum was rejected (not searched)
     const uint32_t *order;// [nspec] spectra, heaviest first
-    uint32_t *queue;      // work-queue head
+    uint32_t *queue;      // work-queue head (two counters: the batched and the pipelined kernel)
+    uint32_t split;       // 1: k_search_batched leaves the spectra k_search_piped takes
     uint32_t *hist_g;     // [nspec * kHist] histograms (always)
     int32_t tile;         // candidates per scorecard tile
     Cell *spill;          // [grid * 32 warps * spill_per_warp] heap entrants of each warp's range

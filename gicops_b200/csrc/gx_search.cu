@@ -521,7 +521,7 @@ extern "C" gx_status gx_workspace_create(const gx_index *ix, uint32_t max_spec, 
     al((void **)&ws->ivl, sizeof(Interval) * 2 * (uint64_t)(max_peaks ? max_peaks : 1));
     al((void **)&ws->nivl, sizeof(uint32_t) * max_spec);
     al((void **)&ws->guard, sizeof(uint32_t) * max_spec);
-    al((void **)&ws->queue, sizeof(uint32_t));
+    al((void **)&ws->queue, 2 * sizeof(uint32_t));
     al((void **)&ws->hist_g, sizeof(uint32_t) * GX_HIST_BINS * (uint64_t)max_spec);
     al((void **)&ws->bs.key_in, sizeof(uint64_t) * max_spec);
     al((void **)&ws->bs.key_out, sizeof(uint64_t) * max_spec);
@@ -535,7 +535,10 @@ extern "C" gx_status gx_workspace_create(const gx_index *ix, uint32_t max_spec, 
         e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (e == cudaSuccess) e = batched_set_attributes(ws->tile);
         ws->bs.sms = sms;
-        for (int c = 1; c <= 3; c++) ws->bs.max_ctas[c] = batched_ctas_per_sm(ws->tile, c);
+        for (int c = 1; c <= 3; c++) {
+            ws->bs.max_ctas[c] = batched_ctas_per_sm(ws->tile, c);
+            ws->bs.piped_ok[c] = piped_fits(ws->tile, c);
+        }
     }
     ws->tiles.tile = ws->tile;
     ws->spill_per_warp = batched_spill_per_warp(ws->tile);
@@ -752,7 +755,8 @@ namespace {
 
 gx_tiles to_c(const BatchedTiles &t)
 {
-    return gx_tiles{(uint32_t)t.chunks, (uint32_t)t.ctas_per_sm, (uint32_t)t.tile, (uint32_t)t.sorted};
+    return gx_tiles{(uint32_t)t.chunks, (uint32_t)t.ctas_per_sm, (uint32_t)t.tile, (uint32_t)t.sorted,
+                    (uint32_t)t.pipeline};
 }
 
 BatchedTiles from_c(const gx_tiles &t)
@@ -762,6 +766,7 @@ BatchedTiles from_c(const gx_tiles &t)
     b.ctas_per_sm = (int)t.ctas_per_sm;
     b.tile = (int)t.tile;
     b.sorted = (int)t.sorted;
+    b.pipeline = (int)t.pipeline;
     return b;
 }
 
@@ -810,9 +815,10 @@ extern "C" gx_status gx_workspace_set_tiles(gx_workspace *ws, const gx_tiles *t)
 {
     if (!ws || !t) return fail(GX_ERR_INVLD_PTR, "gx_workspace_set_tiles: null argument");
     const BatchedTiles b = from_c(*t);
-    if (!batched_tiles_valid(b, ws->tile))
+    if (!batched_tiles_valid(b, ws->tile) || (b.pipeline && !ws->bs.piped_ok[b.chunks]))
         return fail(GX_ERR_INVLD_PARAM, "gx_workspace_set_tiles: chunks_per_lane 1..3, ctas_per_sm 1..2, tile a "
-                                        "multiple of 32 in 1024.." + std::to_string(ws->tile) + ", sorted 0 or 1");
+                                        "multiple of 32 in 1024.." + std::to_string(ws->tile) + ", sorted 0 or 1, "
+                                        "pipeline 0 or 1 (1 only with the whole block as the tile, where it fits)");
     ws->tiles = b;
     return GX_SUCCESS;
 }
@@ -860,6 +866,18 @@ extern "C" gx_status gx_autotune(gx_index *ix, gx_workspace *ws, const gx_querie
                     if (k <= ws->bs.max_ctas[c] && batched_tiles_valid(b, ws->tile) && cand.size() < GX_TUNE_MAX)
                         cand.push_back(b);
                 }
+    // the pipelined kernel (whole blocks as tiles; the batched kernel's share at two CTAs per SM)
+    for (int c = 1; c <= 3; c++)
+        for (int so = 1; so >= 0; so--) {
+            BatchedTiles b;
+            b.chunks = c;
+            b.ctas_per_sm = 2;
+            b.tile = ws->tile;
+            b.sorted = so;
+            b.pipeline = 1;
+            if (ws->bs.piped_ok[c] && batched_tiles_valid(b, ws->tile) && cand.size() < GX_TUNE_MAX)
+                cand.push_back(b);
+        }
     const BatchedTiles keep = ws->tiles;
     std::vector<cudaEvent_t> ev(reps + 1);
     for (auto &e : ev) GX_CUDA(cudaEventCreate(&e));

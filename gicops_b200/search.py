@@ -96,7 +96,7 @@ class Searcher:
 
     @tiles.setter
     def tiles(self, t: dict) -> None:
-        c = N.Tiles(t["chunks_per_lane"], t["ctas_per_sm"], t["tile"], t["sorted"])
+        c = N.Tiles(t["chunks_per_lane"], t["ctas_per_sm"], t["tile"], t["sorted"], t.get("pipeline", 0))
         N.check(N.lib().gx_workspace_set_tiles(self.handle, C.byref(c)))
 
     def autotune(self, q_dev: dict, params: SearchParams, reps: int = 3, use_cache: bool = True,

@@ -254,13 +254,18 @@ gx_status gx_workspace_free(gx_workspace *ws);
  * chunk), 1..3; ctas_per_sm: persistent CTAs per SM, each on its own spectrum, 1..2;
  * tile: candidates per shared-memory scorecard tile (the scorecard partition width), a
  * multiple of 32 from 1024 to the index's block of 11,264 entries; sorted: 1 takes the
- * spectra heaviest first (a sort by scan volume), 0 in batch order.  Results do not
- * depend on the shape.  A new workspace starts at {2, 2, 11264, 1}. */
+ * spectra heaviest first (a sort by scan volume), 0 in batch order; pipeline: 1 runs the
+ * spectra with the 8-byte scorecard and at most 256 bin intervals through the pipelined
+ * kernel (one CTA of 32 warps per SM, one tile scored while the next streams into a second
+ * scorecard; ctas_per_sm then applies to the others).  Results do not depend on the shape.
+ * A new workspace starts at {2, 2, 11264, 1, 0}. */
 typedef struct {
     uint32_t chunks_per_lane;
     uint32_t ctas_per_sm;
     uint32_t tile;
     uint32_t sorted;
+    uint32_t pipeline;            /* 1: one CTA of 32 warps per SM with two scorecard tiles, scoring one
+                                   * tile while streaming the next (tile = the whole block only) */
 } gx_tiles;
 /* CUDA graphs for the batched path's launch sequence (on = 1; 0 releases them).  The
  * sequence (k_prep, sort, k_search_batched, k_tailfit, learned tail) is captured on the
@@ -281,7 +286,7 @@ typedef struct {
     float ms[GX_TUNE_MAX];        /* median of `reps` timed searches of the sample, per candidate */
 } gx_tune_result;
 /* Times every candidate shape (chunks 1-3 x CTAs per SM 1-2 x tile {block, 3/4 block} x
- * sorted or not) on the sample q_dev (device buffers: a few thousand spectra of the
+ * sorted or not, and the pipelined kernel with chunks 1-3, sorted or not) on the sample q_dev (device buffers: a few thousand spectra of the
  * workload), one warm-up and `reps` timed searches each on `stream`, sets the fastest on
  * the workspace and caches it for the workload shape (index, tolerance or per-spectrum
  * tolerances, dF, min_shp, heap capacity, flags, maxz).  With use_cache, a cached choice

@@ -1,7 +1,9 @@
 """The batched path's launch shape and its autotuner (gx_workspace_set_tiles, gx_autotune):
 every candidate shape gives byte-identical results on a multi-block workload, the tuner
 keeps the fastest of the candidates it timed, a second call for the same workload shape
-takes the cached choice, and invalid shapes are refused."""
+takes the cached choice, and invalid shapes are refused.  The shapes include the pipelined
+kernel (two scorecard tiles per CTA), which takes the spectra with the 8-byte scorecard while
+the batched kernel takes the 12-byte ones in the same search."""
 
 import numpy as np
 import pytest
@@ -33,20 +35,19 @@ def setup():
 def test_every_shape_gives_the_same_results(setup):
     gx, torch, s, q, p, qd, keep = setup
     default = s.tiles
-    assert default == {"chunks_per_lane": 2, "ctas_per_sm": 2, "tile": 11264, "sorted": 1}
+    assert default == {"chunks_per_lane": 2, "ctas_per_sm": 2, "tile": 11264, "sorted": 1, "pipeline": 0}
     ref = s.search(q, p, heap=True, hist=True)
-    n = 0
-    for c in (1, 2, 3):
-        for k in (1, 2):
-            for tile in (11264, 8448, 4096):
-                for so in (1, 0):
-                    s.tiles = dict(chunks_per_lane=c, ctas_per_sm=k, tile=tile, sorted=so)
-                    r = s.search(q, p, heap=True, hist=True)
-                    assert r.result.tobytes() == ref.result.tobytes(), (c, k, tile, so)
-                    assert r.heap.tobytes() == ref.heap.tobytes() and np.array_equal(r.hist, ref.hist)
-                    n += 1
+    shapes = [dict(chunks_per_lane=c, ctas_per_sm=k, tile=tile, sorted=so, pipeline=0)
+              for c in (1, 2, 3) for k in (1, 2) for tile in (11264, 8448, 4096) for so in (1, 0)]
+    shapes += [dict(chunks_per_lane=c, ctas_per_sm=k, tile=11264, sorted=so, pipeline=1)
+               for c in (1, 2, 3) for k in (1, 2) for so in (1, 0)]
+    for t in shapes:
+        s.tiles = t
+        r = s.search(q, p, heap=True, hist=True)
+        assert r.result.tobytes() == ref.result.tobytes(), t
+        assert r.heap.tobytes() == ref.heap.tobytes() and np.array_equal(r.hist, ref.hist), t
     s.tiles = default
-    assert n == 36
+    assert len(shapes) == 48
 
 
 def test_autotune_keeps_the_fastest_and_caches_it(setup):
@@ -59,12 +60,12 @@ def test_autotune_keeps_the_fastest_and_caches_it(setup):
     fastest = r["candidates"][int(np.argmin(ms))]
     assert r["best"] == {k: fastest[k] for k in r["best"]}
     assert s.tiles == r["best"]
-    s.tiles = {"chunks_per_lane": 1, "ctas_per_sm": 1, "tile": 4096, "sorted": 0}
+    s.tiles = {"chunks_per_lane": 1, "ctas_per_sm": 1, "tile": 4096, "sorted": 0, "pipeline": 0}
     r2 = s.autotune(qd, p, reps=3, use_cache=True, stream=stream)
     assert r2["cached"] and r2["best"] == r["best"] and s.tiles == r["best"]
     # results with the chosen shape equal the default's
     out = s.search(q, p)
-    s.tiles = {"chunks_per_lane": 2, "ctas_per_sm": 2, "tile": 11264, "sorted": 1}
+    s.tiles = {"chunks_per_lane": 2, "ctas_per_sm": 2, "tile": 11264, "sorted": 1, "pipeline": 0}
     assert s.search(q, p).result.tobytes() == out.result.tobytes()
 
 
@@ -75,7 +76,9 @@ def test_invalid_shapes_are_refused(setup):
                 {"chunks_per_lane": 2, "ctas_per_sm": 3, "tile": 11264, "sorted": 1},
                 {"chunks_per_lane": 2, "ctas_per_sm": 2, "tile": 11296, "sorted": 1},
                 {"chunks_per_lane": 2, "ctas_per_sm": 2, "tile": 1000, "sorted": 1},
-                {"chunks_per_lane": 2, "ctas_per_sm": 2, "tile": 2048, "sorted": 2}):
+                {"chunks_per_lane": 2, "ctas_per_sm": 2, "tile": 2048, "sorted": 2},
+                {"chunks_per_lane": 2, "ctas_per_sm": 2, "tile": 8448, "sorted": 1, "pipeline": 1},
+                {"chunks_per_lane": 2, "ctas_per_sm": 2, "tile": 11264, "sorted": 1, "pipeline": 2}):
         with pytest.raises(gx.GxError) as e:
             s.tiles = bad
         assert e.value.code == -3002

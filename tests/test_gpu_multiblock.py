@@ -10,6 +10,7 @@ golden cases (one block, one tile per length) never reach:
 * spectra with more than 256 merged bin intervals (span tables built per 256-interval
   chunk, offsets not carried), in the 8-byte and in the 12-byte scorecard;
 * the plain path's candidate tiles after the first 8,192 entries of a window;
+* the pipelined kernel (two scorecard tiles per CTA) over the same windows;
 * per-spectrum precursor tolerances (half the spectra at +-10 ppm).
 
 The comparison is the same as for the golden cases (conftest.assert_same): counts,
@@ -78,11 +79,14 @@ def searched():
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("maxz", [1, 2])
-@pytest.mark.parametrize("flags", [0, 1, 2], ids=["default", "wide", "plain"])
+@pytest.mark.parametrize("flags", [0, 1, 2, "piped"], ids=["default", "wide", "plain", "piped"])
 def test_gpu_multiblock(gx, searched, maxz, flags):
     H, q, nmany, o, oh = searched(maxz)
     dev = gx.DeviceIndex(H, 0)
     s = gx.Searcher(dev, q.n, len(q.moz))
+    if flags == "piped":   # the pipelined kernel for the 8-byte spectra, the batched one for the rest
+        s.tiles = dict(s.tiles, pipeline=1)
+        flags = 0
     r = s.search(q, gx.SearchParams(dM=DM, expect_max=1e300, flags=flags), heap=True, hist=True)
     assert_same(r.result, r.heap, r.hist, o, oh, None)
     assert not np.any(r.result["status"] & 4)
@@ -92,7 +96,7 @@ def test_gpu_multiblock(gx, searched, maxz, flags):
     elif flags == 0:
         # the many-interval spectra: 8-byte scorecard at maxz 1, 12-byte at maxz 2
         assert np.all(wide[-nmany:] == (maxz >= 2))
-    assert (o["status"] & 1).sum() > 0.9 * q.n
+    assert (o["status"] & 1).sum() > 0.7 * q.n   # +-10 ppm spectra at maxz 1 often have < 4 candidate PSMs
 
 
 @pytest.mark.gpu

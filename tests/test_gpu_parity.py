@@ -25,12 +25,15 @@ def gx():
 
 
 @pytest.mark.parametrize("case", CASES)
-@pytest.mark.parametrize("flags", [0, 1, 2], ids=["default", "wide", "plain"])
+@pytest.mark.parametrize("flags", [0, 1, 2, "piped"], ids=["default", "wide", "plain", "piped"])
 def test_gpu_golden(gx, golden, case, flags):
     c = golden(case)
     H, q = c["index"], c["queries"]
     dev = gx.DeviceIndex(H, 0)
     s = gx.Searcher(dev, q.n, len(q.moz))
+    if flags == "piped":
+        s.tiles = dict(s.tiles, pipeline=1)
+        flags = 0
     r = s.search(q, search_params(c, flags=flags), heap=True, hist=True)
     ores, ohist = pyoracle.search(H.lengths, q, oracle_params(c), hist=True)
     assert_same(r.result, r.heap, r.hist, ores, ohist, c)
