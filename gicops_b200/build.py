@@ -26,7 +26,7 @@ HOSTCXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "--expt-relaxed-constexpr",
            "-Xcompiler", "-fPIC,-fopenmp,-ffp-contract=off", "-ccbin", HOSTCXX, "-I" + os.path.join(ROOT, "include")]
-# extra nvcc flags, e.g. GX_NVCC_FLAGS="-DGX_SCAN_PAIRS=1" (recorded next to the library, so
+# extra nvcc flags, e.g. GX_NVCC_FLAGS="-DGX_PEND=192" (recorded next to the library, so
 # that a change of flags rebuilds it)
 EXTRA = os.environ.get("GX_NVCC_FLAGS", "").split()
 STAMP = os.path.join(OUT, "nvcc_flags.txt")

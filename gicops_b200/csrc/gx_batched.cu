@@ -209,13 +209,7 @@ static_assert(kIvlChunk <= 256, "the warp search covers 32 x 8 span-table entrie
 #ifndef GX_FUSED_CLEAR
 #define GX_FUSED_CLEAR 1   // packed scorecard reset during the scan and after scoring (0: one pass after)
 #endif
-#ifndef GX_SCAN_PAIRS
-#define GX_SCAN_PAIRS 0    // packed scan: lane l reads candidate pairs 2l and 64 + 2l of each 128 (contiguous 16-byte loads)
-#endif
-#ifndef GX_LOG_TABLE
-#define GX_LOG_TABLE 1     // log10 of intensity sums from the device-filled table (0: log10 at each use)
-#endif
-static_assert(!(GX_SCAN_PAIRS && !GX_FUSED_CLEAR), "the pair scan resets the scorecard as it goes");
+
 
 // Dynamic shared memory after the scorecard tile (tile * 8 bytes):
 //   dummy      kDummy words right after the scorecard, written and never read
@@ -333,13 +327,8 @@ __device__ __forceinline__ void score_batch(SM &sm, const uint32_t *pend, const 
     for (int g = 0; g < kG; g++) {
         // log10 of small integers from a table filled by the same log10 (identical values)
         const uint32_t xb = 1u + ib[g], xy = 1u + iy[g];
-#if GX_LOG_TABLE
         lb[g] = xb < a.logtab_n ? __ldg(a.logtab + xb) : log10((double)xb);
         ly[g] = xy < a.logtab_n ? __ldg(a.logtab + xy) : log10((double)xy);
-#else
-        lb[g] = log10((double)xb);
-        ly[g] = log10((double)xy);
-#endif
     }
 #pragma unroll
     for (int g = 0; g < kG; g++) {
@@ -386,19 +375,14 @@ __device__ __forceinline__ void score_batch(SM &sm, const uint32_t *pend, const 
     }
 }
 
-// Resets the packed-scorecard groups of the n scored candidates in q (four candidates,
-// 32 bytes; with the pair scan two candidates, 16 bytes): the scan left every group
-// holding a PSM as it was, for the scoring.
+// Resets the packed-scorecard groups (four candidates, 32 bytes) of the n scored
+// candidates in q: the scan left every group holding a PSM as it was, for the scoring.
 __device__ __forceinline__ void clear_scored(uint32_t *sw, const uint32_t *q, int n, int lane)
 {
     for (int i = lane; i < n; i += 32) {
-#if GX_SCAN_PAIRS
-        *reinterpret_cast<uint4 *>(sw + 2 * (q[i] & ~1u)) = make_uint4(0u, 0u, 0u, 0u);
-#else
         uint4 *z = reinterpret_cast<uint4 *>(sw + 2 * (q[i] & ~3u));
         z[0] = make_uint4(0u, 0u, 0u, 0u);
         z[1] = make_uint4(0u, 0u, 0u, 0u);
-#endif
     }
 }
 
@@ -815,53 +799,6 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
                 for (int c0 = r0; c0 < r1; c0 += step) {
                     unsigned m = 0;
                     int cb;
-#if GX_SCAN_PAIRS
-                    if (!wide) {
-                        // lane l: candidates ca, ca + 1 (ca = c0 + 2l) and cc, cc + 1 (cc = c0 + 64 + 2l):
-                        // each 16-byte load of the warp covers 512 contiguous bytes
-                        const int ca = c0 + 2 * lane, cc = ca + 64;
-                        if (ca < r1) {
-                            uint4 *z = reinterpret_cast<uint4 *>(sw + 2 * ca);
-                            const uint4 v = *z;
-                            const unsigned ma = ((((v.x >> 24) + (v.y >> 24)) >= minshp) ? 1u : 0u) |
-                                                ((((v.z >> 24) + (v.w >> 24)) >= minshp && ca + 1 < r1) ? 2u : 0u);
-                            if (ma == 0u) *z = make_uint4(0u, 0u, 0u, 0u);
-                            m = ma;
-                        }
-                        if (cc < r1) {
-                            uint4 *z = reinterpret_cast<uint4 *>(sw + 2 * cc);
-                            const uint4 v = *z;
-                            const unsigned mb = ((((v.x >> 24) + (v.y >> 24)) >= minshp) ? 1u : 0u) |
-                                                ((((v.z >> 24) + (v.w >> 24)) >= minshp && cc + 1 < r1) ? 2u : 0u);
-                            if (mb == 0u) *z = make_uint4(0u, 0u, 0u, 0u);
-                            m |= mb << 2;
-                        }
-                        const unsigned lt = (1u << lane) - 1u;
-                        const unsigned B0 = __ballot_sync(0xffffffffu, m & 1u), B1 = __ballot_sync(0xffffffffu, m & 2u);
-                        const unsigned B2 = __ballot_sync(0xffffffffu, m & 4u), B3 = __ballot_sync(0xffffffffu, m & 8u);
-                        const int half = __popc(B0) + __popc(B1);
-                        const int total = half + __popc(B2) + __popc(B3);
-                        if (total == 0) continue;
-                        if (npend + total > kPend) {   // queue full: score what it holds first
-                            __syncwarp();
-                            score_batch<BatchSmem, kEntSmem>(sm, dd.pend[wid], a, scv, ctile, wid, lane, npend, t0, ixx, speclen, tau, wide, ent,
-                                                      nent, cps);
-                            __syncwarp();
-                            clear_scored(sw, dd.pend[wid], npend, lane);
-                            npend = 0;
-                            __syncwarp();
-                        }
-                        // queue positions in candidate order: the first 64 candidates, then the next 64
-                        int pa = npend + __popc(B0 & lt) + __popc(B1 & lt);
-                        int pb = npend + half + __popc(B2 & lt) + __popc(B3 & lt);
-                        if (m & 1u) dd.pend[wid][pa++] = (uint32_t)ca;
-                        if (m & 2u) dd.pend[wid][pa] = (uint32_t)(ca + 1);
-                        if (m & 4u) dd.pend[wid][pb++] = (uint32_t)cc;
-                        if (m & 8u) dd.pend[wid][pb] = (uint32_t)(cc + 1);
-                        npend += total;
-                        continue;
-                    }
-#endif
                     if (!wide) {
                         // lane l: candidates cb .. cb + 3 (cb = c0 + 4l), words b, y, b, y, b, y, b, y
                         cb = c0 + 4 * lane;
