@@ -875,9 +875,9 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
                 }
                 // warp 0 prepares the next tile's span table (the others are still scoring)
                 if (wid == 0) {
-                    if (ti + 1 < nsub) {          // next sub-tile of this block: same table
-                        if (lane == 0) { sm.next_unit = 0; sm.ready = 1u; }
-                    } else if (niA) {
+                    if (ti + 1 < nsub && carry) {   // next sub-tile of this block: the same table, when one
+                        if (lane == 0) { sm.next_unit = 0; sm.ready = 1u; }   // table holds every interval
+                    } else if (ti + 1 >= nsub && niA) {
                         build_span_warp(sm, dd, nv, nrel0, lane);
                         if (lane == 0) sm.ready = 1u;
                     } else if (lane == 0) {

@@ -6,7 +6,9 @@ golden cases (one block, one tile per length) never reach:
 * windows over two or more 11,264-entry blocks in the batched kernel, with the next
   block's bin offsets loaded one tile ahead and its span table built while the current
   tile is scored;
-* the 12-byte scorecard's second sub-tile of a block (the same span table, restreamed);
+* the 12-byte scorecard's second sub-tile of a block (the same span table, restreamed), and
+  narrower tiles (several sub-tiles per block in either scorecard), with more than 256
+  intervals too (the span table rebuilt per 256-interval chunk for every sub-tile);
 * spectra with more than 256 merged bin intervals (span tables built per 256-interval
   chunk, offsets not carried), in the 8-byte and in the 12-byte scorecard;
 * the plain path's candidate tiles after the first 8,192 entries of a window;
@@ -79,13 +81,16 @@ def searched():
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("maxz", [1, 2])
-@pytest.mark.parametrize("flags", [0, 1, 2, "piped"], ids=["default", "wide", "plain", "piped"])
+@pytest.mark.parametrize("flags", [0, 1, 2, "piped", "narrow"], ids=["default", "wide", "plain", "piped", "narrow"])
 def test_gpu_multiblock(gx, searched, maxz, flags):
     H, q, nmany, o, oh = searched(maxz)
     dev = gx.DeviceIndex(H, 0)
     s = gx.Searcher(dev, q.n, len(q.moz))
     if flags == "piped":   # the pipelined kernel for the 8-byte spectra, the batched one for the rest
         s.tiles = dict(s.tiles, pipeline=1)
+        flags = 0
+    elif flags == "narrow":   # tiles of 4,096 candidates: several sub-tiles per block in both scorecards
+        s.tiles = dict(s.tiles, tile=4096)
         flags = 0
     r = s.search(q, gx.SearchParams(dM=DM, expect_max=1e300, flags=flags), heap=True, hist=True)
     assert_same(r.result, r.heap, r.hist, o, oh, None)
