@@ -650,9 +650,9 @@ def main():
         t0 = time.perf_counter()
         tr = ws.autotune(tqd, params, reps=3, use_cache=False, stream=stream.cuda_stream)
         tiles = {"chosen": tr["best"], "sample": int(len(sel)), "tune_s": round(time.perf_counter() - t0, 2),
-                 "candidates_ms": [[c["chunks_per_lane"], c["ctas_per_sm"], c["tile"], c["sorted"], round(c["ms"], 3)]
-                                   for c in tr["candidates"]],
-                 "candidate_fields": ["chunks_per_lane", "ctas_per_sm", "tile", "sorted", "ms"]}
+                 "candidates_ms": [[c["chunks_per_lane"], c["ctas_per_sm"], c["tile"], c["sorted"], c["pipeline"],
+                                    round(c["ms"], 3)] for c in tr["candidates"]],
+                 "candidate_fields": ["chunks_per_lane", "ctas_per_sm", "tile", "sorted", "pipeline", "ms"]}
         log(f"[bench] autotuned launch shape: {tr['best']} ({tiles['tune_s']} s)")
         del tqd, tkeep
 
