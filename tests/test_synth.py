@@ -48,3 +48,20 @@ def test_pbin_roundtrip(tmp_path):
     assert np.array_equal(r.prec, q.prec) and np.array_equal(r.charge, q.charge)
     s = q.subset([3, 1])
     assert s.n == 2 and np.array_equal(s.moz[: s.idx[1]], q.moz[q.idx[3]:q.idx[4]])
+
+
+def test_concat_keeps_spectra_and_offsets():
+    import gicops_b200 as gx
+    db = gx.synth.make_database(60, seed=3)
+    H = gx.HostIndex.build(db, maxz=1, ions=False)
+    a = gx.synth.make_queries(H.entries_by_len(), 7, seed=1, window="mixed")
+    b = gx.synth.make_queries(H.entries_by_len(), 5, seed=2)
+    c = gx.synth.QueryBatch.concat([a, b])
+    assert c.n == 12 and c.idx[0] == 0 and c.idx[-1] == len(a.moz) + len(b.moz)
+    for i in range(a.n):
+        assert np.array_equal(c.moz[c.idx[i]:c.idx[i + 1]], a.moz[a.idx[i]:a.idx[i + 1]])
+    for i in range(b.n):
+        j = a.n + i
+        assert np.array_equal(c.intn[c.idx[j]:c.idx[j + 1]], b.intn[b.idx[i]:b.idx[i + 1]])
+    assert np.array_equal(c.prec, np.concatenate([a.prec, b.prec]))
+    assert np.array_equal(np.isnan(c.dM[a.n:]), np.ones(b.n, bool))   # b had no per-spectrum tolerances

@@ -113,3 +113,22 @@ def test_adam_matches_closed_form_first_step():
     P1, m, v = T.adam(P, G, np.zeros(5), np.zeros(5), step=1, lr=0.01)
     # first step: m/bc1 = g, v/bc2 = g^2, so the move is lr * sign(g) (up to eps)
     np.testing.assert_allclose(P1, 1 - 0.01 * np.sign(G) * np.abs(G) / (np.abs(G) + 1e-8), rtol=1e-12)
+
+
+def test_choose_sparse_below_takes_the_largest_winning_threshold():
+    """The fallback threshold: the largest candidate count below which the learned line
+    beats the plain fit on both the median and the 90th percentile; 0 when it never does."""
+    import gicops_b200.tail as T
+    rng = np.random.default_rng(0)
+    cands = rng.integers(20, 500, 4000)
+    ep = rng.exponential(5.0, 4000)
+    el = np.where(cands < 150, 0.5 * ep, 2.0 * ep)          # learned wins below 150 only
+    t = T.choose_sparse_below(ep, el, cands)
+    ths = (25, 50, 75, 100, 150, 200, 300, 500)
+    wins = lambda x: (np.median(el[cands < x]) < np.median(ep[cands < x]) and  # noqa: E731
+                      np.quantile(el[cands < x], 0.9) < np.quantile(ep[cands < x], 0.9))
+    assert t >= 150 and wins(t) and not any(wins(x) for x in ths if x > t)
+    assert T.choose_sparse_below(ep, 2.0 * ep, cands) == 0   # never wins
+    assert T.choose_sparse_below(ep, 0.5 * ep, cands) == 500
+    # too few rows below a threshold: that threshold is not judged
+    assert T.choose_sparse_below(ep[:50], 0.5 * ep[:50], cands[:50]) == 0
