@@ -206,6 +206,9 @@ constexpr int kEntSmem = GX_ENT_SMEM;   // heap entrants per warp kept in shared
 #define GX_WARP_SEARCH 1   // a unit's first interval found by a two-level warp search (0: binary search)
 #endif
 static_assert(kIvlChunk <= 256, "the warp search covers 32 x 8 span-table entries");
+#ifndef GX_STREAM_PREFETCH
+#define GX_STREAM_PREFETCH 0   // stream: the next unit's chunks loaded before the current one's are scattered
+#endif
 #ifndef GX_FUSED_CLEAR
 #define GX_FUSED_CLEAR 1   // packed scorecard reset during the scan and after scoring (0: one pass after)
 #endif
@@ -553,6 +556,85 @@ __device__ __forceinline__ void stream_tile(BatchSmem &sm, const BatchDyn &dd, c
     uint32_t *cnt = reinterpret_cast<uint32_t *>(scv);
     const uint32_t dummy = 2u * (uint32_t)ctile + (uint32_t)lane;   // packed: words [2T, 2T + 32)
     const uint32_t fill = whole ? (dummy | (dummy << 16)) : 0xFFFFFFFFu;
+#if GX_STREAM_PREFETCH
+    // The next unit's chunks are located and loaded before the current unit's ids are
+    // scattered, so that the loads' latency overlaps the scatter.
+    auto claim = [&]() -> uint32_t {
+        uint32_t u = 0;
+        if (lane == 0) u = atomicAdd(&sm.next_unit, 1u);
+        return __shfl_sync(0xffffffffu, u, 0) * (32u * CH);
+    };
+    auto locate_load = [&](uint32_t j0, uint32_t (&kx)[CH], uint4 (&v)[CH]) {
+        const uint32_t s1 = (uint32_t)lane * 8u;
+        const uint32_t b1 = __ballot_sync(0xffffffffu, s1 < ncv && dd.sp_pre[s1] <= j0);
+        const uint32_t base = (31u - (uint32_t)__clz(b1)) * 8u;
+        const uint32_t s2 = base + ((uint32_t)lane & 7u);
+        const uint32_t b2 = __ballot_sync(0xffffffffu, lane < 8 && s2 < ncv && dd.sp_pre[s2] <= j0);
+        uint32_t k = base + (31u - (uint32_t)__clz(b2));
+#pragma unroll
+        for (int p = 0; p < CH; p++) {
+            const uint32_t j = j0 + (uint32_t)lane + 32u * p;
+            kx[p] = 0xFFFFFFFFu;
+            if (j < M) {
+                while (dd.sp_pre[k + 1] <= j) k++;
+                kx[p] = k;
+                v[p] = __ldg(ia4 + (dd.sp_rec[k].x + j));
+            }
+        }
+    };
+    uint32_t j0 = claim();
+    uint4 v[CH];
+    uint32_t kx[CH];
+    if (j0 < M) locate_load(j0, kx, v);
+    while (j0 < M) {
+        const uint32_t jn = claim();
+        uint4 vn[CH];
+        uint32_t kn[CH];
+        if (jn < M) locate_load(jn, kn, vn);
+#pragma unroll
+        for (int p = 0; p < CH; p++) {
+            if (kx[p] == 0xFFFFFFFFu) continue;
+            const uint4 r = dd.sp_rec[kx[p]];
+            const uint32_t j = j0 + (uint32_t)lane + 32u * p;
+            const uint32_t eq = (r.x + j) << 3;
+            if (!wide) {
+                const uint32_t mlo = r.y > eq ? r.y - eq : 0u;
+                const uint32_t mhi = min(r.z - eq, 8u);
+                const uint4 kl = sm.keep_lo[mlo], kh = sm.keep_hi[mhi - 1u];
+                uint32_t w4[4] = {v[p].x, v[p].y, v[p].z, v[p].w};
+                const uint32_t km[4] = {kl.x & kh.x, kl.y & kh.y, kl.z & kh.z, kl.w & kh.w};
+#pragma unroll
+                for (int q = 0; q < 4; q++) w4[q] = (w4[q] & km[q]) | (fill & ~km[q]);
+                if (whole) {
+#pragma unroll
+                    for (int m = 0; m < 8; m++) atomicAdd(cnt + ((w4[m >> 1] >> (16 * (m & 1))) & 0xFFFFu), r.w);
+                } else {
+#pragma unroll
+                    for (int m = 0; m < 8; m++)
+                        scatter_packed(cnt, (w4[m >> 1] >> (16 * (m & 1))) & 0xFFFFu, lo, lim, r.w, dummy, true);
+                }
+            } else {
+                const uint32_t c = dd.sp_c[kx[p]];
+                const uint32_t w4[4] = {v[p].x, v[p].y, v[p].z, v[p].w};
+                const bool full = eq >= r.y && eq + 8u <= r.z;
+#pragma unroll
+                for (int m = 0; m < 8; m++) {
+                    const uint32_t e = eq + (uint32_t)m;
+                    if (full || (e >= r.y && e < r.z))
+                        scatter_wide(cnt, cnt + ctile, cnt + 2 * ctile, (w4[m >> 1] >> (16 * (m & 1))) & 0xFFFFu, lo,
+                                     lim, c, r.w);
+                }
+            }
+        }
+        j0 = jn;
+#pragma unroll
+        for (int p = 0; p < CH; p++) {
+            v[p] = vn[p];
+            kx[p] = kn[p];
+        }
+    }
+    return;
+#endif
     for (;;) {
         uint32_t u = 0;
         if (lane == 0) u = atomicAdd(&sm.next_unit, 1u);
