@@ -10,6 +10,10 @@
 //                   of every interval (each bucket read once) into the BYC scorecard in
 //                   shared memory, then scan the tile in entry order (hyperscore,
 //                   histogram, exact top-K heap)
+//   k_search_piped  (launch-shape option) one CTA of 32 warps per SM with two scorecard
+//                   tiles: tile t scored while tile t + 1 streams, one barrier per tile; it
+//                   takes the 8-byte-scorecard spectra of at most 256 intervals and
+//                   k_search_batched the others
 //   k_tailfit       one warp per spectrum: expeRT tail fit and e-value
 //
 // Results are identical to the reference's CPU path (source/core/dslim_query.cpp:
