@@ -133,6 +133,8 @@ _SIGS = [
     ("gx_index_upload", C.c_int32, [C.POINTER(LengthDesc), C.c_int32, C.c_uint32, C.c_int32, C.POINTER(C.c_void_p)]),
     ("gx_index_free", C.c_int32, [C.c_void_p]),
     ("gx_index_bytes", C.c_uint64, [C.c_void_p]),
+    ("gx_index_save", C.c_int32, [C.c_void_p, C.c_char_p]),
+    ("gx_index_load", C.c_int32, [C.c_char_p, C.c_int32, C.POINTER(C.c_void_p)]),
     ("gx_build_length", C.c_int32, [C.c_char_p, C.c_uint32, C.c_uint32, C.POINTER(BuildParams),
                                     C.POINTER(C.c_void_p)]),
     ("gx_host_length_desc", C.c_int32, [C.c_void_p, C.POINTER(LengthDesc)]),

@@ -16,6 +16,7 @@ fragment ions, the CSR and the block layout on the GPU from the host entries
 from __future__ import annotations
 
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -155,6 +156,20 @@ class DeviceIndex:
             if not has_csr:
                 raise ValueError("the host index has no CSR (built with ions=False): use on_device")
             N.check(N.lib().gx_index_upload(host.descs(), host.nlen, host.nbins, device, C.byref(self.handle)))
+
+    def save(self, path: str) -> None:
+        """Write the device arrays to a file (gx_index_save)."""
+        N.check(N.lib().gx_index_save(self.handle, os.fsencode(path)))
+
+    @classmethod
+    def load(cls, path: str, device: int = 0, host: "HostIndex | None" = None) -> "DeviceIndex":
+        """An index written by save(), put back on `device` without building (gx_index_load).
+        `host` (optional) is the HostIndex it was built from, for read_length and the
+        peptide strings of results."""
+        obj = cls.__new__(cls)
+        obj.host, obj.device, obj.handle = host, device, C.c_void_p()
+        N.check(N.lib().gx_index_load(os.fsencode(path), device, C.byref(obj.handle)))
+        return obj
 
     def read_length(self, i: int) -> dict:
         """Device arrays of length i: bA, iA (ids 2*entry + (y ion)), iAb (block-local), mass."""

@@ -81,6 +81,15 @@ gx_status gx_index_upload(const gx_length_desc *lens, int32_t nlen, uint32_t nbi
 gx_status gx_index_free(gx_index *ix);
 /* bytes held in HBM by an index */
 uint64_t gx_index_bytes(const gx_index *ix);
+/* Write a device index to a file, every array as the device holds it, and load such a file
+ * onto a device without building anything (the large configuration's 27 GB index takes 20 s
+ * to build from host arrays).  The file records the library's entry-block size and layout
+ * version; a file of another layout, a truncated file or one of another kind is refused
+ * (GX_ERR_INVLD_INDEX, GX_ERR_NOT_ENOUGH_DATA).  Copies go through a 64 MB pinned buffer.
+ * No counterpart in the reference, which rebuilds its index in every run and caches only
+ * preprocessed spectra (source/core/msquery.cpp:542-721). */
+gx_status gx_index_save(const gx_index *ix, const char *path);
+gx_status gx_index_load(const char *path, int32_t device, gx_index **out);
 
 /* ---- host index builder (LBE_CountPeps/Initialize + MODS_GenerateMods + DSLIM_Construct) */
 typedef struct {
