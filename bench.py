@@ -774,8 +774,8 @@ def main():
     if os.path.exists(tf):
         tj = json.load(open(tf))
         ent = tj.get(args.workload, {}).get(top_k)
-        if ent:
-            traffic = ent["dram_bytes_per_launch"]
+        if ent:   # per launch of the workload's whole batch; a --spectra case scales by spectra
+            traffic = ent["dram_bytes_per_launch"] * q.n / ent["launch_spectra"]
 
     # ---- parity of the benchmarked outputs (untimed) --------------------------------
     parity = None
