@@ -201,7 +201,10 @@ constexpr int kDummy = 32;      // scorecard words that take the adds of ids out
 // 16-byte id chunks each lane loads per work unit before it scatters any: a template
 // parameter of the kernel (1..kMaxChunks), chosen per launch (BatchedTiles::chunks)
 constexpr int kMaxChunks = 3;
-constexpr int kHeapWarp = kBWarps - 1;      // inserts heap entrants while the others stream
+// The last warp inserts heap entrants while the others stream, and builds the next tile's
+// span table while the others scan and score (it takes no share of the scan).
+constexpr int kHeapWarp = kBWarps - 1;
+constexpr int kScanWarps = kBWarps - 1;
 #ifndef GX_ENT_SMEM
 #define GX_ENT_SMEM 8
 #endif
@@ -784,7 +787,7 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
         int cps = 0;   // candidate PSMs counted by this warp (lane 0 adds them at the end)
         bool heap_due = false;
         // Offsets of the next tile's bins, loaded by thread i for interval i one tile ahead
-        // (when all intervals fit one span table): warp 0 builds that tile's span table from
+        // (when all intervals fit one span table): the last warp builds that tile's span table from
         // them while the others score.
         uint32_t nx_s = 0, nx_e = 0;
         int nx_len = -1;
@@ -873,13 +876,14 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
                     }
                     __syncthreads();
                 }
-                // ---- scan: warp w owns candidates [w*R, (w+1)*R) and takes them in entry ----
-                // order, four per lane per step, queues those that reach min_shp and scores the
-                // queue when it is full and at the end; then clears its range for the next tile
+                // ---- scan: warp w < kScanWarps owns candidates [w*R, (w+1)*R) and takes them ----
+                // in entry order, four per lane per step, queues those that reach min_shp and
+                // scores the queue when it is full and at the end; then clears its range for
+                // the next tile.  Warp kHeapWarp builds the next tile's span table meanwhile.
                 const float tau = sm.heap_size < a.heap_cap ? -1.0f : sm.root;
                 const int step = wide ? 32 : 128;
-                const int R = ((tn + kBWarps - 1) / kBWarps + step - 1) / step * step;
-                const int r0 = min(tn, wid * R), r1 = min(tn, r0 + R);
+                const int R = ((tn + kScanWarps - 1) / kScanWarps + step - 1) / step * step;
+                const int r0 = wid < kScanWarps ? min(tn, wid * R) : tn, r1 = min(tn, r0 + R);
                 int npend = 0, nent = 0;
                 uint32_t *sw = reinterpret_cast<uint32_t *>(scv);
                 for (int c0 = r0; c0 < r1; c0 += step) {
@@ -959,8 +963,8 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
                         }
                     }
                 }
-                // warp 0 prepares the next tile's span table (the others are still scoring)
-                if (wid == 0) {
+                // the last warp prepares the next tile's span table (the others are still scoring)
+                if (wid == kHeapWarp) {
                     if (ti + 1 < nsub && carry) {   // next sub-tile of this block: the same table, when one
                         if (lane == 0) { sm.next_unit = 0; sm.ready = 1u; }   // table holds every interval
                     } else if (ti + 1 >= nsub && niA) {
