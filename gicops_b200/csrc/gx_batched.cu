@@ -205,6 +205,12 @@ constexpr int kMaxChunks = 3;
 // span table while the others scan and score (it takes no share of the scan).
 constexpr int kHeapWarp = kBWarps - 1;
 constexpr int kScanWarps = kBWarps - 1;
+// Candidates of a tile of tn that each scanning warp owns (a multiple of the scan step): at
+// most the length of the warp's entrant list.
+__host__ __device__ constexpr int scan_range(int tn, int step)
+{
+    return ((tn + kScanWarps - 1) / kScanWarps + step - 1) / step * step;
+}
 #ifndef GX_ENT_SMEM
 #define GX_ENT_SMEM 8
 #endif
@@ -882,7 +888,7 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
                 // the next tile.  Warp kHeapWarp builds the next tile's span table meanwhile.
                 const float tau = sm.heap_size < a.heap_cap ? -1.0f : sm.root;
                 const int step = wide ? 32 : 128;
-                const int R = ((tn + kScanWarps - 1) / kScanWarps + step - 1) / step * step;
+                const int R = scan_range(tn, step);
                 const int r0 = wid < kScanWarps ? min(tn, wid * R) : tn, r1 = min(tn, r0 + R);
                 int npend = 0, nent = 0;
                 uint32_t *sw = reinterpret_cast<uint32_t *>(scv);
@@ -1023,6 +1029,9 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
 // of them); k_search_batched takes the rest in a second launch.
 // ------------------------------------------------------------------------------------
 constexpr int kPWarps = 32;
+// Candidates of a tile of tn that each warp of k_search_piped scans (a multiple of 128): at
+// most the length of the warp's entrant list of one tile parity.
+__host__ __device__ constexpr int piped_range(int tn) { return ((tn + kPWarps - 1) / kPWarps + 127) / 128 * 128; }
 constexpr int kPBlock = kPWarps * 32;
 constexpr int kPPend = 136;                  // per-warp queue: one scan step (128) + slack
 constexpr int kPHeapWarp = kPWarps - 1;
@@ -1354,7 +1363,7 @@ __global__ void __launch_bounds__(kPBlock, 1) k_search_piped(SearchArgs a)
                 // ---- scan and score tile p - 1: warp w owns [w R, (w + 1) R), four candidates per lane per step
                 const float tau = *reinterpret_cast<volatile float *>(&sm.tau);
                 const int tn = ts.tn;
-                const int R = ((tn + kPWarps - 1) / kPWarps + 127) / 128 * 128;
+                const int R = piped_range(tn);
                 const int r0 = min(tn, wid * R), r1 = min(tn, r0 + R);
                 uint32_t *sw = dd.card[bs];
                 uint32_t *pend = dd.pend[wid];
@@ -1556,8 +1565,11 @@ int batched_ctas_per_sm(int tile, int chunks)
 // Largest candidate range of one warp in a tile (its entrants never exceed it).
 uint32_t batched_spill_per_warp(int tile)
 {
-    const int step = 128;
-    return (uint32_t)(((tile + kBWarps - 1) / kBWarps + step - 1) / step * step);
+    // the largest range of k_search_batched: the 8-byte scorecard's (step 128) over the whole
+    // tile (the 12-byte scorecard's ranges, step 32 over two thirds of it, are shorter); and
+    // k_search_piped's, which keeps two lists (one per tile parity) in the same space
+    const int r = scan_range(tile, 128), rp = 2 * piped_range(tile);
+    return (uint32_t)(r > rp ? r : rp);
 }
 
 cudaError_t batched_set_attributes(int tile)
