@@ -4,9 +4,9 @@ A database of 3,000 length-20 peptides that share their first 15 residues: a spe
 of the shared b ions matches every one of them with at least 15 ions, so in the first tile
 of each spectrum (the heap not yet full) every candidate enters the heap.  Each warp of the
 batched kernel then keeps one entrant per candidate of its range, the longest entrant lists
-the kernel can produce; the narrow tiles (1,952 and 4,096 candidates) are the sizes whose
-ranges are longest relative to the tile.  Counts, histograms and heap arrays must be
-bit-exact against the oracle, as in the golden cases.
+the kernel can produce, at the default tile and at two narrower ones (several sub-tiles per
+block).  Counts, histograms and heap arrays must be bit-exact against the oracle, as in the
+golden cases.
 """
 
 import numpy as np
