@@ -26,6 +26,7 @@
 #include "../../include/gicops_b200.h"
 #include "gx_batched.h"
 #include "gx_device.cuh"
+#include "gx_index.cuh"
 #include "gx_internal.h"
 
 namespace gx {
@@ -797,7 +798,7 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
         // them while the others score.
         uint32_t nx_s = 0, nx_e = 0;
         int nx_len = -1;
-        int64_t nx_kb = -1;
+        int nx_kb = -1;
         const bool carry = nv <= (uint32_t)kIvlChunk;
 
         for (int ixx = 0; ixx < a.nlen; ixx++) {
@@ -808,19 +809,18 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
             const uint32_t rel0 = (uint32_t)(ln.ia_off - base);
             const uint4 *__restrict__ ia4 = reinterpret_cast<const uint4 *>(a.iAb + base);
             const uint32_t speclen = ln.speclen;
-            const int64_t E = a.block;
-            const int64_t kb0 = w.x / E, kb1 = w.y / E;
-            for (int64_t kb = kb0; kb <= kb1; kb++) {
+            constexpr int E = kBlockEntries;   // the index's block (launch_batched checks a.block)
+            const int kb0 = w.x / E, kb1 = w.y / E;
+            for (int kb = kb0; kb <= kb1; kb++) {
               // one block of entries = one candidate tile (two sub-tiles for the wide scorecard)
               const uint32_t *__restrict__ bA = a.blkA + ln.blk_off + (uint64_t)kb * (a.nbins + 1);
-              const int bt0 = (int)max((int64_t)w.x, kb * E), bt1 = (int)min((int64_t)w.y + 1, (kb + 1) * E);
+              const int bt0 = max(w.x, kb * E), bt1 = min(w.y + 1, (kb + 1) * E);
               const int nsub = (bt1 - bt0 + ctile - 1) / ctile;
               const bool have = carry && nx_len == ixx && nx_kb == kb;   // offsets loaded a tile ago
               const uint32_t cur_s = nx_s, cur_e = nx_e;
               // the next tile of this spectrum: the next block of this length, or the first
               // block of the next length with a window
-              int nx = -1;
-              int64_t nkb = 0;
+              int nx = -1, nkb = 0;
               if (kb < kb1) {
                   nx = ixx;
                   nkb = kb + 1;
@@ -834,18 +834,15 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
                       }
                   }
               }
-              const uint16_t *niA = nullptr;
-              uint32_t nrel0 = 0;
-              if (carry && nx >= 0) {
-                  const DevLen nl = a.lens[nx];
-                  niA = a.iAb + nl.ia_off;
-                  nrel0 = (uint32_t)(nl.ia_off & 7ull);
-                  if (tid < (int)nv) {
-                      const uint32_t *nbA = a.blkA + nl.blk_off + (uint64_t)nkb * (a.nbins + 1);
-                      const Interval v = ivl[tid];
-                      nx_s = __ldg(nbA + v.b0);      // in flight while this tile streams
-                      nx_e = __ldg(nbA + v.b1 + 1);
-                  }
+              // (the next length's offsets are loaded only by the threads that use them: the
+              // interval threads now, the last warp for the next span table after the scan)
+              const bool has_next = carry && nx >= 0;
+              if (has_next && tid < (int)nv) {
+                  const uint64_t nblk = nx == ixx ? ln.blk_off : a.lens[nx].blk_off;
+                  const uint32_t *nbA = a.blkA + nblk + (uint64_t)nkb * (a.nbins + 1);
+                  const Interval v = ivl[tid];
+                  nx_s = __ldg(nbA + v.b0);      // in flight while this tile streams
+                  nx_e = __ldg(nbA + v.b1 + 1);
               }
               nx_len = nx;
               nx_kb = nkb;
@@ -856,7 +853,7 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
                 if (tn <= 0) continue;
                 const uint32_t lo = 2u * (uint32_t)(t0 - kb * E), lim = 2u * (uint32_t)tn;
                 // the tile is the whole block (all its entries): every id of the block is a word of it
-                const bool whole = !wide && (int64_t)t0 == kb * E && (int64_t)t1 == min((kb + 1) * E, (int64_t)ln.npep);
+                const bool whole = !wide && t0 == kb * E && t1 == min((kb + 1) * E, (int)ln.npep);
                 // ---- stream every interval's ids into the scorecard ----------------------
                 const bool prebuilt = sm.ready != 0u;   // built while the last tile was scored
                 for (uint32_t ic0 = 0; ic0 < nv; ic0 += kIvlChunk) {
@@ -876,7 +873,7 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
                         heap_due = false;
                     }
                     stream_tile<CH>(sm, dd, ia4, ncv, scv, ctile, wide, whole, lo, lim, lane);
-                    if (ti == 0 && niA && tid < (int)nv) {   // the next tile's offsets, for its span table
+                    if (ti == 0 && has_next && tid < (int)nv) {   // the next tile's offsets, for its span table
                         dd.nx_s[tid] = nx_s;
                         dd.nx_e[tid] = nx_e;
                     }
@@ -973,8 +970,9 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
                 if (wid == kHeapWarp) {
                     if (ti + 1 < nsub && carry) {   // next sub-tile of this block: the same table, when one
                         if (lane == 0) { sm.next_unit = 0; sm.ready = 1u; }   // table holds every interval
-                    } else if (ti + 1 >= nsub && niA) {
-                        build_span_warp(sm, dd, nv, nrel0, lane);
+                    } else if (ti + 1 >= nsub && has_next) {
+                        const uint64_t nia = nx == ixx ? ln.ia_off : a.lens[nx].ia_off;
+                        build_span_warp(sm, dd, nv, (uint32_t)(nia & 7ull), lane);
                         if (lane == 0) sm.ready = 1u;
                     } else if (lane == 0) {
                         sm.ready = 0u;
@@ -1591,6 +1589,7 @@ bool batched_tiles_valid(const BatchedTiles &t, int max_tile)
 cudaError_t launch_batched(SearchArgs a, const BatchedScratch &b, const BatchedTiles &t, cudaStream_t st)
 {
     cudaError_t e;
+    if (a.block != (uint32_t)kBlockEntries) return cudaErrorInvalidValue;   // k_search_batched's tile arithmetic
     a.tile = t.tile;
     int h = prof_begin("k_prep", st);
     k_prep<<<a.nspec, kPrepBlock, 0, st>>>(a, const_cast<int2 *>(a.win), b.key_in, b.ord_in);
