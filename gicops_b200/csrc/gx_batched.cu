@@ -900,9 +900,10 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
                             const uint4 qb = *reinterpret_cast<const uint4 *>(sw + 2 * cb + 4);
                             const int lim4 = r1 - cb;   // candidates of the four inside the range
                             m = ((((qa.x >> 24) + (qa.y >> 24)) >= minshp) ? 1u : 0u) |
-                                ((((qa.z >> 24) + (qa.w >> 24)) >= minshp && lim4 > 1) ? 2u : 0u) |
-                                ((((qb.x >> 24) + (qb.y >> 24)) >= minshp && lim4 > 2) ? 4u : 0u) |
-                                ((((qb.z >> 24) + (qb.w >> 24)) >= minshp && lim4 > 3) ? 8u : 0u);
+                                ((((qa.z >> 24) + (qa.w >> 24)) >= minshp) ? 2u : 0u) |
+                                ((((qb.x >> 24) + (qb.y >> 24)) >= minshp) ? 4u : 0u) |
+                                ((((qb.z >> 24) + (qb.w >> 24)) >= minshp) ? 8u : 0u);
+                            if (lim4 < 4) m &= (1u << lim4) - 1u;
 #if GX_FUSED_CLEAR
                             if (m == 0u) {   // no PSM among the four: reset them for the next tile now
                                 uint4 *z = reinterpret_cast<uint4 *>(sw + 2 * cb);
@@ -918,11 +919,13 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
                             m = (((cv & 0xFFFFu) + (cv >> 16)) & 0xFFFFu) >= minshp ? 1u : 0u;
                         }
                     }
-                    // queue positions: lane order, then candidate order inside the lane
+                    // queue positions: lane order, then candidate order inside the lane; the
+                    // lanes' counts (0..4) by their three bits, one ballot each
                     const unsigned lt = (1u << lane) - 1u;
-                    const unsigned B0 = __ballot_sync(0xffffffffu, m & 1u), B1 = __ballot_sync(0xffffffffu, m & 2u);
-                    const unsigned B2 = __ballot_sync(0xffffffffu, m & 4u), B3 = __ballot_sync(0xffffffffu, m & 8u);
-                    const int total = __popc(B0) + __popc(B1) + __popc(B2) + __popc(B3);
+                    const unsigned nm = (unsigned)__popc(m);
+                    const unsigned B0 = __ballot_sync(0xffffffffu, nm & 1u), B1 = __ballot_sync(0xffffffffu, nm & 2u);
+                    const unsigned B2 = __ballot_sync(0xffffffffu, nm & 4u);
+                    const int total = __popc(B0) + 2 * __popc(B1) + 4 * __popc(B2);
                     if (total == 0) continue;
                     if (npend + total > kPend) {   // queue full: score what it holds first
                         __syncwarp();
@@ -933,7 +936,7 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
                         npend = 0;
                         __syncwarp();
                     }
-                    int pos = npend + __popc(B0 & lt) + __popc(B1 & lt) + __popc(B2 & lt) + __popc(B3 & lt);
+                    int pos = npend + __popc(B0 & lt) + 2 * __popc(B1 & lt) + 4 * __popc(B2 & lt);
                     for (unsigned mm = m; mm; mm &= mm - 1u) dd.pend[wid][pos++] = (uint32_t)(cb + __ffs(mm) - 1);
                     npend += total;
                 }
