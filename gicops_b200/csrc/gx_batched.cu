@@ -206,6 +206,7 @@ constexpr int kMaxChunks = 3;
 // span table while the others scan and score (it takes no share of the scan).
 constexpr int kHeapWarp = kBWarps - 1;
 constexpr int kScanWarps = kBWarps - 1;
+constexpr int kUnitTab = 64;   // stream units whose first interval the warp-built span table records
 // Candidates of a tile of tn that each scanning warp owns (a multiple of the scan step): at
 // most the length of the warp's entrant list.
 __host__ __device__ constexpr int scan_range(int tn, int step)
@@ -279,11 +280,13 @@ struct BatchSmem {
     uint32_t next_unit;
     uint32_t ent_mask;               // warps with entrants in the last scored tile
     uint32_t ready;                  // the span table of the next tile is built
+    uint32_t unit_n;                 // stream units whose first interval unit_k holds (0: none)
     float root;
     // keep masks of a 16-byte chunk's eight ids: keep_lo[m] keeps ids m.., keep_hi[m]
     // keeps ids ..m (index m - 1)
     uint4 keep_lo[8];
     uint4 keep_hi[8];
+    uint8_t unit_k[kUnitTab];        // interval of the first chunk of each of the first stream units
 };
 
 // Block-local ids are 2*(entry - block start) + (y ion); the tile's ids satisfy
@@ -477,7 +480,10 @@ __device__ __forceinline__ void build_span_table(BatchSmem &sm, const BatchDyn &
         dd.sp_rec[tid] = make_uint4(0u, a0, a1, wide ? v.S : ((v.c << 24) | v.S));
         dd.sp_c[tid] = v.c;
     }
-    if (tid == 0) sm.next_unit = 0;
+    if (tid == 0) {
+        sm.next_unit = 0;
+        sm.unit_n = 0;   // the stream finds each unit's first interval by search
+    }
     // block exclusive scan of cnt
     uint32_t x = cnt;
 #pragma unroll
@@ -508,7 +514,9 @@ __device__ __forceinline__ void build_span_table(BatchSmem &sm, const BatchDyn &
 
 // The span table of the next tile, built by one warp from the offsets in nx_s / nx_e
 // while the other warps score (the adds of the spectrum's intervals, record field w and
-// sp_c, stay in place); it also resets the unit counter.
+// sp_c, stay in place); it also resets the unit counter and records the interval of the first
+// chunk of each of the first kUnitTab stream units (units of 32 x CH chunks).
+template <int CH>
 __device__ __forceinline__ void build_span_warp(BatchSmem &sm, const BatchDyn &dd, uint32_t n, uint32_t rel0, int lane)
 {
     constexpr int kPer = kIvlChunk / 32;
@@ -537,12 +545,16 @@ __device__ __forceinline__ void build_span_warp(BatchSmem &sm, const BatchDyn &d
         if (lane >= o) incl += y;
     }
     uint32_t run = incl - sum;
+    constexpr uint32_t U = 32u * CH;
 #pragma unroll
     for (int j = 0; j < kPer; j++) {
         const uint32_t i = i0 + j;
         if (i < n) {
             dd.sp_pre[i] = run;
             dd.sp_rec[i].x = q0s[j] - run;
+            // the units that start inside this interval's chunks [run, run + cnt)
+            const uint32_t ue = min((run + cnt[j] + U - 1u) / U, (uint32_t)kUnitTab);
+            for (uint32_t u = (run + U - 1u) / U; u < ue; u++) sm.unit_k[u] = (uint8_t)i;
         }
         run += cnt[j];
     }
@@ -550,6 +562,7 @@ __device__ __forceinline__ void build_span_warp(BatchSmem &sm, const BatchDyn &d
     if (lane == 0) {
         dd.sp_pre[n] = total;
         sm.next_unit = 0;
+        sm.unit_n = min((total + U - 1u) / U, (uint32_t)kUnitTab);
     }
 }
 
@@ -656,8 +669,12 @@ __device__ __forceinline__ void stream_tile(BatchSmem &sm, const BatchDyn &dd, c
         const uint32_t j0 = u * (32u * CH);
         if (j0 >= M) break;
         // interval of the unit's first chunk (the last k < ncv with pre[k] <= j0, a non-empty
-        // interval: pre is non-decreasing, pre[0] = 0 and pre[ncv] > j0); each lane walks on
-        // from there
+        // interval: pre is non-decreasing, pre[0] = 0 and pre[ncv] > j0), recorded by the span
+        // table's builder for the first units; each lane walks on from there
+        uint32_t k;
+        if (u < sm.unit_n) {
+            k = sm.unit_k[u];
+        } else {
 #if GX_WARP_SEARCH
         // two levels across the warp: every 8th entry, then the 8 entries of that group
         const uint32_t s1 = (uint32_t)lane * 8u;
@@ -665,14 +682,16 @@ __device__ __forceinline__ void stream_tile(BatchSmem &sm, const BatchDyn &dd, c
         const uint32_t base = (31u - (uint32_t)__clz(b1)) * 8u;
         const uint32_t s2 = base + ((uint32_t)lane & 7u);
         const uint32_t b2 = __ballot_sync(0xffffffffu, lane < 8 && s2 < ncv && dd.sp_pre[s2] <= j0);
-        uint32_t k = base + (31u - (uint32_t)__clz(b2));
+        k = base + (31u - (uint32_t)__clz(b2));
 #else
-        uint32_t k = 0, hi = ncv;
+        k = 0;
+        uint32_t hi = ncv;
         while (hi - k > 1) {
             const uint32_t mid = (k + hi) >> 1;
             if (dd.sp_pre[mid] <= j0) k = mid; else hi = mid;
         }
 #endif
+        }
         uint4 v[CH];
         uint32_t kx[CH];
 #pragma unroll
@@ -975,7 +994,7 @@ __global__ void __launch_bounds__(kBBlock, kCtasPerSm) k_search_batched(SearchAr
                         if (lane == 0) { sm.next_unit = 0; sm.ready = 1u; }   // table holds every interval
                     } else if (ti + 1 >= nsub && has_next) {
                         const uint64_t nia = nx == ixx ? ln.ia_off : a.lens[nx].ia_off;
-                        build_span_warp(sm, dd, nv, (uint32_t)(nia & 7ull), lane);
+                        build_span_warp<CH>(sm, dd, nv, (uint32_t)(nia & 7ull), lane);
                         if (lane == 0) sm.ready = 1u;
                     } else if (lane == 0) {
                         sm.ready = 0u;
