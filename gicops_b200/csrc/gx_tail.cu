@@ -247,6 +247,13 @@ struct GemmArgs {
 constexpr int kGemmThreads = 128;
 constexpr int kKStage = 64;
 constexpr int kATileBytes = 128 * kKStage * 2;
+constexpr int kBufBytes = kATileBytes + 256 * kKStage * 2;   // one stage: the A tile and a B tile of NT <= 256
+// Dynamic shared memory of every k_gemm CTA: two operand stages of at most 48 KB (the next
+// k-step's operands are copied in while the tensor core reads the current ones), within a
+// request that lets at most two CTAs share an SM, whose 512 TMEM columns then always cover
+// their two allocations of at most 256 columns.
+constexpr int kGemmSmem = 100 * 1024;
+static_assert(2 * kBufBytes <= kGemmSmem, "two operand stages");
 // After a wait has given up, the kernel still waits this long for the MMA it issued last
 // (it reads the operand tiles and writes the TMEM that the kernel frees afterwards).
 constexpr uint64_t kDrainNs = 1000000000ull;
@@ -259,9 +266,20 @@ __device__ __forceinline__ float gelu_grad(float z)
     return cdf + z * pdf;
 }
 
+// 16-byte asynchronous copy global -> shared of src_bytes (0..16) bytes, the rest zero.
+__device__ __forceinline__ void cp_async16(uint8_t *dst, const void *src, uint32_t src_bytes)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(mma::smem_addr(dst)), "l"(src), "r"(src_bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
 // Stage rows [r0, r0+R) x k [k0, k0+64) of a strided bf16 matrix into the no-swizzle
 // K-major core-matrix layout: 16-byte row (r, kc) at ((kc*(R/8) + r/8)*128 + (r%8)*16).
-// Out-of-range rows and k are zero.
+// Out-of-range rows and k are zero.  A row's 16 bytes that are contiguous and aligned in
+// global memory travel by an asynchronous copy (complete after cp_async_wait_all), the
+// others (strided operands, unaligned rows) by plain loads and stores.
 __device__ __forceinline__ void stage_tile(uint8_t *sm, int R, const bf16 *g, long long sr, long long sk, int r0,
                                            int nr, int k0, int nk)
 {
@@ -273,10 +291,12 @@ __device__ __forceinline__ void stage_tile(uint8_t *sm, int R, const bf16 *g, lo
         else { r = u % R; kc = u / R; }
         uint4 v = make_uint4(0u, 0u, 0u, 0u);
         const int kb = kc * 8;
+        uint8_t *dst = sm + (kc * (R >> 3) + (r >> 3)) * 128 + (r & 7) * 16;
         if (r < nr && kb < nk) {
             const bf16 *p = g + (long long)(r0 + r) * sr + (long long)(k0 + kb) * sk;
-            if (kfast && kb + 8 <= nk && ((reinterpret_cast<uintptr_t>(p) & 15u) == 0)) {
-                v = *reinterpret_cast<const uint4 *>(p);
+            if (kfast && ((reinterpret_cast<uintptr_t>(p) & 15u) == 0)) {
+                cp_async16(dst, p, 2u * (uint32_t)min(8, nk - kb));
+                continue;
             } else {
                 uint16_t e[8];
 #pragma unroll
@@ -288,7 +308,44 @@ __device__ __forceinline__ void stage_tile(uint8_t *sm, int R, const bf16 *g, lo
                 v.w = e[6] | ((uint32_t)e[7] << 16);
             }
         }
-        *reinterpret_cast<uint4 *>(sm + (kc * (R >> 3) + (r >> 3)) * 128 + (r & 7) * 16) = v;
+        *reinterpret_cast<uint4 *>(dst) = v;
+    }
+}
+
+// Sixteen consecutive columns of one row when the whole group is inside the matrix and the
+// outputs (and Z) allow 16-byte accesses: the same values as the element-wise epilogue, in
+// 16-byte stores (four for fp32, two for bf16).
+__device__ __forceinline__ void epilogue16(const GemmArgs &a, int row, int col0, const float (&v)[16])
+{
+    float z[16];
+    if (a.epi == kEpiDGelu) {
+        const float4 *zp = reinterpret_cast<const float4 *>(a.Z + (long long)row * a.ldz + col0);
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const float4 t = zp[q];
+            z[4 * q] = t.x; z[4 * q + 1] = t.y; z[4 * q + 2] = t.z; z[4 * q + 3] = t.w;
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < 16; j++) z[j] = a.epi == kEpiF32 ? v[j] : v[j] + a.bias[col0 + j];
+    }
+    if (a.epi != kEpiDGelu) {
+        float4 *dp = reinterpret_cast<float4 *>(a.D + (long long)row * a.ldd + col0);
+#pragma unroll
+        for (int q = 0; q < 4; q++) dp[q] = make_float4(z[4 * q], z[4 * q + 1], z[4 * q + 2], z[4 * q + 3]);
+    }
+    if (a.epi == kEpiBiasGelu || a.epi == kEpiDGelu) {
+        uint32_t h[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const float f0 = a.epi == kEpiBiasGelu ? gelu(z[2 * j]) : v[2 * j] * gelu_grad(z[2 * j]);
+            const float f1 = a.epi == kEpiBiasGelu ? gelu(z[2 * j + 1]) : v[2 * j + 1] * gelu_grad(z[2 * j + 1]);
+            h[j] = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(f0)) |
+                   ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(f1)) << 16);
+        }
+        uint4 *hp = reinterpret_cast<uint4 *>(a.H + (long long)row * a.ldh + col0);
+        hp[0] = make_uint4(h[0], h[1], h[2], h[3]);
+        hp[1] = make_uint4(h[4], h[5], h[6], h[7]);
     }
 }
 
@@ -324,16 +381,15 @@ __device__ __forceinline__ void epilogue(const GemmArgs &a, int row, int col0, c
 __global__ void __launch_bounds__(kGemmThreads) k_gemm(GemmArgs a)
 {
     extern __shared__ __align__(1024) uint8_t dsm[];
-    __shared__ uint64_t bar;
+    __shared__ uint64_t bar[2];   // completion of the MMAs that read stage 0 / stage 1
     __shared__ uint32_t tmem_base;
-    uint8_t *sA = dsm;
-    uint8_t *sB = dsm + kATileBytes;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int m0 = blockIdx.x * 128, n0 = blockIdx.y * a.NT;
     const uint32_t ncols = a.NT <= 32 ? 32u : a.NT <= 64 ? 64u : a.NT <= 128 ? 128u : 256u;
     if (warp == 0) mma::tmem_alloc(&tmem_base, ncols);
     if (tid == 0) {
-        mma::mbar_init(&bar, 1);
+        mma::mbar_init(&bar[0], 1);
+        mma::mbar_init(&bar[1], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     mma::fence_before_sync();
@@ -341,44 +397,85 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(GemmArgs a)
     mma::fence_after_sync();
     const uint32_t tmem = tmem_base;
     const uint32_t idesc = mma::idesc_bf16_f32(128, (uint32_t)a.NT);
-    const uint32_t sa = mma::smem_addr(sA), sb = mma::smem_addr(sB);
     const uint32_t a_lbo = 16 * 128, b_lbo = (uint32_t)(a.NT / 8) * 128;
-    uint32_t phase = 0;
-    bool ok = true;
-    for (int k0 = 0; k0 < a.K; k0 += kKStage) {
+    const int nks = (a.K + kKStage - 1) / kKStage;
+    // stage s of k-step ks: A tile at dsm + s * kBufBytes, B tile after it
+    auto stage = [&](int st, int k0) {
+        uint8_t *sA = dsm + st * kBufBytes;
         stage_tile(sA, 128, a.A, a.sam, a.sak, m0, a.M - m0, k0, a.K - k0);
-        stage_tile(sB, a.NT, a.B, a.sbn, a.sbk, n0, a.N - n0, k0, a.K - k0);
+        stage_tile(sA + kATileBytes, a.NT, a.B, a.sbn, a.sbk, n0, a.N - n0, k0, a.K - k0);
+        cp_async_commit();
+    };
+    uint32_t ph = 0u;     // bit b: the phase of barrier b that its next wait expects
+    uint32_t pend = 0u;   // bit b: an MMA commit on barrier b not yet waited for
+    bool ok = true;
+    stage(0, 0);
+    for (int ks = 0; ks < nks; ks++) {
+        const int st = ks & 1;
+        cp_async_wait_all();   // this thread's copies of stage st (the only ones in flight)
         mma::fence_smem_to_async();
         __syncthreads();
         if (tid == 0) {
             mma::fence_after_sync();
+            const uint32_t sa = mma::smem_addr(dsm + st * kBufBytes), sb = sa + (uint32_t)kATileBytes;
+            const int k0 = ks * kKStage;
             const int steps = min(kKStage / 16, (a.K - k0 + 15) / 16);
-            for (int s = 0; s < steps; s++) {
-                const uint64_t da = mma::desc_kmajor(sa + (uint32_t)s * 2 * a_lbo, a_lbo, 128);
-                const uint64_t db = mma::desc_kmajor(sb + (uint32_t)s * 2 * b_lbo, b_lbo, 128);
-                mma::mma_bf16(tmem, da, db, idesc, (k0 | s) != 0);
+            for (int s2 = 0; s2 < steps; s2++) {
+                const uint64_t da = mma::desc_kmajor(sa + (uint32_t)s2 * 2 * a_lbo, a_lbo, 128);
+                const uint64_t db = mma::desc_kmajor(sb + (uint32_t)s2 * 2 * b_lbo, b_lbo, 128);
+                mma::mma_bf16(tmem, da, db, idesc, (k0 | s2) != 0);
             }
-            mma::mma_commit(&bar);
+            mma::mma_commit(&bar[st]);
         }
-        // the tiles are restaged next round: wait for the tensor core to finish reading
-        ok = mma::mbar_wait(&bar, phase, a.wait_ns);
-        phase ^= 1u;
-        if (__syncthreads_or(!ok)) {   // uniform: the warp-wide TMEM loads below need it
-            ok = false;
-            break;
+        pend |= 1u << st;
+        if (ks + 1 < nks) {
+            // the other stage was read by the MMAs of k-step ks - 1: wait for them, then copy
+            // k-step ks + 1 into it while the tensor core works on stage st
+            const int o = st ^ 1;
+            if (pend & (1u << o)) {
+                const bool w = mma::mbar_wait(&bar[o], (ph >> o) & 1u, a.wait_ns);
+                if (w) {
+                    ph ^= 1u << o;
+                    pend &= ~(1u << o);
+                }
+                if (__syncthreads_or(!w)) {   // uniform: every thread leaves the loop together
+                    ok = false;
+                    break;
+                }
+            }
+            stage(o, (ks + 1) * kKStage);
         }
+    }
+    if (ok) {   // the last k-step's MMAs
+        const int st = (nks - 1) & 1;
+        const bool w = mma::mbar_wait(&bar[st], (ph >> st) & 1u, a.wait_ns);
+        if (w) {
+            ph ^= 1u << st;
+            pend &= ~(1u << st);
+        }
+        if (__syncthreads_or(!w)) ok = false;
     }
     if (!ok) {
         if (tid == 0 && a.err) atomicExch(a.err, 2);
-        mma::mbar_wait(&bar, phase ^ 1u, kDrainNs);   // the outstanding commit, bounded
+        // the commits not yet observed (each barrier has at most one), bounded
+        for (int b = 0; b < 2; b++)
+            if (pend & (1u << b)) mma::mbar_wait(&bar[b], (ph >> b) & 1u, kDrainNs);
+        cp_async_wait_all();
     } else {
         mma::fence_after_sync();
         const int row = m0 + warp * 32 + lane;
         const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+        // 16-byte stores need the outputs (and Z) 16-byte aligned at every row
+        const bool vec = (a.epi == kEpiDGelu || (((uintptr_t)a.D & 15u) == 0 && (a.ldd & 3) == 0)) &&
+                         (a.epi < kEpiBiasGelu || (((uintptr_t)a.H & 15u) == 0 && (a.ldh & 7) == 0)) &&
+                         (a.epi != kEpiDGelu || (((uintptr_t)a.Z & 15u) == 0 && (a.ldz & 3) == 0));
         for (int c = 0; c < a.NT; c += 16) {
             float v[16];
             mma::tmem_ld16(trow + (uint32_t)c, v);
-            if (row < a.M) epilogue(a, row, n0 + c, v);
+            if (row < a.M) {
+                if (vec && n0 + c + 16 <= a.N) epilogue16(a, row, n0 + c, v);
+                else epilogue(a, row, n0 + c, v);
+            }
         }
     }
     mma::fence_before_sync();
@@ -526,11 +623,6 @@ bool g_attr_done[64] = {};
 constexpr uint64_t kDefaultWaitNs = 1000000000ull;
 std::atomic<uint64_t> g_wait_ns{kDefaultWaitNs};
 
-// Dynamic shared memory of every k_gemm CTA.  The operand tiles need at most 48 KB; the
-// request is padded so that at most two CTAs share an SM, whose 512 TMEM columns then
-// always cover their two allocations of at most 256 columns.
-constexpr int kGemmSmem = 100 * 1024;
-static_assert(kATileBytes + 256 * kKStage * 2 <= kGemmSmem, "operand tiles");
 
 gx_status set_attributes(int device)
 {
