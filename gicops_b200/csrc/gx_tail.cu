@@ -244,7 +244,7 @@ struct GemmArgs {
     uint64_t wait_ns;     // limit of each wait for the tensor core (global-timer nanoseconds)
 };
 
-constexpr int kGemmThreads = 128;
+constexpr int kGemmThreads = 256;   // two warps per TMEM lane quarter in the epilogue
 constexpr int kKStage = 64;
 constexpr int kATileBytes = 128 * kKStage * 2;
 constexpr int kBufBytes = kATileBytes + 256 * kKStage * 2;   // one stage: the A tile and a B tile of NT <= 256
@@ -463,13 +463,15 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(GemmArgs a)
         cp_async_wait_all();
     } else {
         mma::fence_after_sync();
-        const int row = m0 + warp * 32 + lane;
-        const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+        // warps w and w + 4 read the same 32 TMEM lanes (rows), alternate 16-column groups
+        const int quarter = warp & 3;
+        const int row = m0 + quarter * 32 + lane;
+        const uint32_t trow = tmem + ((uint32_t)(quarter * 32) << 16);
         // 16-byte stores need the outputs (and Z) 16-byte aligned at every row
         const bool vec = (a.epi == kEpiDGelu || (((uintptr_t)a.D & 15u) == 0 && (a.ldd & 3) == 0)) &&
                          (a.epi < kEpiBiasGelu || (((uintptr_t)a.H & 15u) == 0 && (a.ldh & 7) == 0)) &&
                          (a.epi != kEpiDGelu || (((uintptr_t)a.Z & 15u) == 0 && (a.ldz & 3) == 0));
-        for (int c = 0; c < a.NT; c += 16) {
+        for (int c = 16 * (warp >> 2); c < a.NT; c += 32) {
             float v[16];
             mma::tmem_ld16(trow + (uint32_t)c, v);
             if (row < a.M) {
